@@ -1,0 +1,171 @@
+"""ctypes access to the CPU oracle (oracle/liboracle.so) for the tests.
+
+The oracle is the checker: the tests compare the CUDA library against it.
+Builds the oracle with make on first use when the shared object is missing.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ODIR = os.path.join(ROOT, "oracle")
+SO = os.path.join(ODIR, "liboracle.so")
+
+OK, INVALID_BUFFER, POS_RANGE, INVALID_BLOCK_LENGTH, INVALID_FLAGS, UNSUPPORTED_TYPE, \
+    NOT_IMPLEMENTED, OVERFLOW = range(8)
+DELTA, NOFOR, NOPATCH, SPECIAL, APPEND, NOINPLACE = 1, 2, 4, 8, 16, 32
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        src = os.path.join(ODIR, "utl_oracle.c")
+        if not os.path.exists(SO) or os.path.getmtime(SO) < os.path.getmtime(src):
+            subprocess.check_call(["make", "-s", "-C", ODIR])
+        L = C.CDLL(SO)
+        P8, PU32, PU64, SZ = C.POINTER(C.c_uint8), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_size_t)
+        PI = C.POINTER(C.c_int)
+        L.utlo_pack_u32.argtypes = [C.c_uint8, PU32, C.c_int, P8, SZ]
+        L.utlo_pack_u64.argtypes = [C.c_uint8, PU64, C.c_int, P8, SZ]
+        L.utlo_unpack_u32.argtypes = [P8, C.c_size_t, PU32, PI, SZ, PI]
+        L.utlo_unpack_u64.argtypes = [P8, C.c_size_t, PU64, PI, SZ, PI]
+        L.utlo_get_u32.argtypes = [C.c_int, P8, C.c_size_t, PU32, PI]
+        L.utlo_get_u64.argtypes = [C.c_int, P8, C.c_size_t, PU64, PI]
+        L.utlo_block_length.argtypes = [P8, C.c_size_t, SZ]
+        L.utlo_header.argtypes = [P8, C.c_size_t] + [PI] * 7
+        L.utlo_max_block_length32.argtypes = [C.c_uint8]
+        L.utlo_max_block_length64.argtypes = [C.c_uint8]
+        L.utlo_stream_pack_bound_u32.argtypes = [C.c_uint8, PU64, C.c_int]
+        L.utlo_stream_pack_bound_u32.restype = C.c_size_t
+        L.utlo_stream_pack_bound_u64.argtypes = [C.c_uint8, PU64, C.c_int]
+        L.utlo_stream_pack_bound_u64.restype = C.c_size_t
+        L.utlo_pack_streams_u32.argtypes = [C.c_uint8, PU32, PU64, C.c_int, P8, C.c_size_t, PU64, PU64, C.c_int]
+        L.utlo_pack_streams_u64.argtypes = [C.c_uint8, PU64, PU64, C.c_int, P8, C.c_size_t, PU64, PU64, C.c_int]
+        L.utlo_unpack_streams_u32.argtypes = [P8, PU64, PU64, C.c_int, PU32, C.c_int]
+        L.utlo_unpack_streams_u64.argtypes = [P8, PU64, PU64, C.c_int, PU64, C.c_int]
+        _lib = L
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def _bytes(src):
+    b = np.frombuffer(bytes(src), dtype=np.uint8).copy()
+    if b.size == 0:
+        b = np.zeros(1, dtype=np.uint8)[:0]
+    return b
+
+
+def pack_u32(flag, values):
+    v = np.ascontiguousarray(values, dtype=np.uint32)
+    dst = np.zeros(2048, dtype=np.uint8)
+    n = C.c_size_t(0)
+    err = lib().utlo_pack_u32(flag, _p(v, C.c_uint32), len(v), _p(dst, C.c_uint8), C.byref(n))
+    return (bytes(dst[:n.value]) if err == 0 else None), err
+
+
+def pack_u64(flag, values):
+    v = np.ascontiguousarray(values, dtype=np.uint64)
+    dst = np.zeros(4096, dtype=np.uint8)
+    n = C.c_size_t(0)
+    err = lib().utlo_pack_u64(flag, _p(v, C.c_uint64), len(v), _p(dst, C.c_uint8), C.byref(n))
+    return (bytes(dst[:n.value]) if err == 0 else None), err
+
+
+def unpack_u32(src):
+    b = _bytes(src)
+    out = np.zeros(128, dtype=np.uint32)
+    cnt, cons, ovf = C.c_int(0), C.c_size_t(0), C.c_int(0)
+    err = lib().utlo_unpack_u32(_p(b, C.c_uint8), len(b), _p(out, C.c_uint32), C.byref(cnt), C.byref(cons), C.byref(ovf))
+    if err:
+        return None, 0, err, ovf.value
+    return out[:cnt.value].copy(), cons.value, 0, 0
+
+
+def unpack_u64(src):
+    b = _bytes(src)
+    out = np.zeros(128, dtype=np.uint64)
+    cnt, cons, ovf = C.c_int(0), C.c_size_t(0), C.c_int(0)
+    err = lib().utlo_unpack_u64(_p(b, C.c_uint8), len(b), _p(out, C.c_uint64), C.byref(cnt), C.byref(cons), C.byref(ovf))
+    if err:
+        return None, 0, err, ovf.value
+    return out[:cnt.value].copy(), cons.value, 0, 0
+
+
+def get_u32(pos, src):
+    b = _bytes(src)
+    v, ovf = C.c_uint32(0), C.c_int(0)
+    err = lib().utlo_get_u32(pos, _p(b, C.c_uint8), len(b), C.byref(v), C.byref(ovf))
+    return (v.value if err == 0 else 0), err, ovf.value
+
+
+def get_u64(pos, src):
+    b = _bytes(src)
+    v, ovf = C.c_uint64(0), C.c_int(0)
+    err = lib().utlo_get_u64(pos, _p(b, C.c_uint8), len(b), C.byref(v), C.byref(ovf))
+    return (v.value if err == 0 else 0), err, ovf.value
+
+
+def block_length(src):
+    b = _bytes(src)
+    n = C.c_size_t(0)
+    err = lib().utlo_block_length(_p(b, C.c_uint8), len(b), C.byref(n))
+    return (n.value if err == 0 else 0), err
+
+
+def header(src):
+    b = _bytes(src)
+    f = [C.c_int(0) for _ in range(7)]
+    err = lib().utlo_header(_p(b, C.c_uint8), len(b), *[C.byref(x) for x in f])
+    return [x.value for x in f], err
+
+
+def max_block_length32(flag):
+    return lib().utlo_max_block_length32(flag)
+
+
+def max_block_length64(flag):
+    return lib().utlo_max_block_length64(flag)
+
+
+def pack_streams(flag, values, val_off, n_threads=4):
+    """Returns (packed bytes ndarray, block_off, stream_byte_off)."""
+    is64 = values.dtype == np.uint64
+    L = lib()
+    vo = np.ascontiguousarray(val_off, dtype=np.uint64)
+    ns = len(vo) - 1
+    bound_fn = L.utlo_stream_pack_bound_u64 if is64 else L.utlo_stream_pack_bound_u32
+    cap = bound_fn(flag, _p(vo, C.c_uint64), ns)
+    out = np.zeros(max(cap, 1), dtype=np.uint8)
+    nb = int(sum((int(vo[s + 1] - vo[s]) + 127) // 128 for s in range(ns)))
+    bo = np.zeros(nb + 1, dtype=np.uint64)
+    so = np.zeros(ns + 1, dtype=np.uint64)
+    if is64:
+        err = L.utlo_pack_streams_u64(flag, _p(values, C.c_uint64), _p(vo, C.c_uint64), ns, _p(out, C.c_uint8), cap,
+                                      _p(bo, C.c_uint64), _p(so, C.c_uint64), n_threads)
+    else:
+        err = L.utlo_pack_streams_u32(flag, _p(values, C.c_uint32), _p(vo, C.c_uint64), ns, _p(out, C.c_uint8), cap,
+                                      _p(bo, C.c_uint64), _p(so, C.c_uint64), n_threads)
+    assert err == 0, err
+    return out[:int(bo[-1])], bo, so
+
+
+def unpack_streams(packed, block_off, val_off, dtype=np.uint32, n_threads=4):
+    L = lib()
+    vo = np.ascontiguousarray(val_off, dtype=np.uint64)
+    bo = np.ascontiguousarray(block_off, dtype=np.uint64)
+    pk = np.ascontiguousarray(packed, dtype=np.uint8)
+    out = np.zeros(int(vo[-1]), dtype=dtype)
+    if dtype == np.uint64:
+        err = L.utlo_unpack_streams_u64(_p(pk, C.c_uint8), _p(bo, C.c_uint64), _p(vo, C.c_uint64), len(vo) - 1,
+                                        _p(out, C.c_uint64), n_threads)
+    else:
+        err = L.utlo_unpack_streams_u32(_p(pk, C.c_uint8), _p(bo, C.c_uint64), _p(vo, C.c_uint64), len(vo) - 1,
+                                        _p(out, C.c_uint32), n_threads)
+    return out, err
