@@ -1,0 +1,237 @@
+/*
+ * utlpfor.h -- C ABI of the B200 (sm_100a) UTL-PFOR block codec.
+ *
+ * Drop-in boundary for the Go package github.com/Akron/utlpfor: each
+ * per-call entry point below is what that package's cgo shim binds in
+ * place of the Go function named beside it (file:line in the reference).
+ * All compute runs on the GPU; there is no CPU code path for pack, unpack
+ * or get.  Header parsing helpers (utl_block_length, utl_header,
+ * utl_max_block_length*) read a few header bytes on the host, as the
+ * reference does.
+ *
+ * Conventions
+ *  - Every function returns a status: 0 on success, else one of UTL_ERR_*.
+ *    Codes 1..7 are the reference's errors (utlpfor.go:70-115); the cgo
+ *    shim maps them back to the same Go error values.
+ *  - Per-call functions take HOST pointers and block until the result is
+ *    back on the host.  They are safe to call from several threads; each
+ *    host thread gets its own CUDA stream and staging buffers on the
+ *    current device.  A utl_codec handle (the Compressor32/64 counterpart)
+ *    carries its own stream and buffers.
+ *  - utl_*_batch_* functions take DEVICE pointers, enqueue work on the
+ *    given cudaStream_t (passed as void*, NULL = legacy default stream) and
+ *    return without synchronizing.  Device buffers must be 16-byte aligned.
+ *  - Streams: stream s of a batch holds values[val_off[s] .. val_off[s+1])
+ *    and packs to ceil(n_s/128) blocks laid out back to back exactly as
+ *    repeated PackUint32(flag|Append, block, dst, ...) calls would lay them
+ *    out (pack.go:76-97); streams follow each other in the packed buffer.
+ *    block_start[s] is the index of stream s's first block (utl_batch_plan).
+ */
+#ifndef UTLPFOR_H
+#define UTLPFOR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define UTL_API __attribute__((visibility("default")))
+#else
+#define UTL_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define UTL_OK 0
+#define UTL_ERR_INVALID_BUFFER 1        /* ErrInvalidBuffer       utlpfor.go:71 */
+#define UTL_ERR_POSITION_OUT_OF_RANGE 2 /* ErrPositionOutOfRange  utlpfor.go:74 */
+#define UTL_ERR_INVALID_BLOCK_LENGTH 3  /* ErrInvalidBlockLength  utlpfor.go:77 */
+#define UTL_ERR_INVALID_FLAGS 4         /* ErrInvalidFlags        utlpfor.go:80 */
+#define UTL_ERR_UNSUPPORTED_TYPE 5      /* ErrUnsupportedType     utlpfor.go:86 */
+#define UTL_ERR_NOT_IMPLEMENTED 6       /* ErrNotImplemented      utlpfor.go:83 */
+#define UTL_ERR_OVERFLOW 7              /* *ErrOverflow{Position} utlpfor.go:108 */
+#define UTL_ERR_COUNT_MISMATCH 8 /* batch: block count/length disagrees with the stream table */
+#define UTL_ERR_CAPACITY 9       /* batch: output buffer too small */
+#define UTL_ERR_TIMEOUT 10       /* device wait gave up (never expected) */
+#define UTL_ERR_ARG 11           /* bad argument (NULL, size, alignment) */
+#define UTL_ERR_CUDA 12          /* CUDA runtime error; see utl_last_cuda_error */
+
+/* ---- flags (utlpfor.go:24-68) ---- */
+#define UTL_DELTA 1
+#define UTL_NOFOR 2
+#define UTL_NOPATCH 4
+#define UTL_SPECIAL 8
+#define UTL_APPEND 16
+#define UTL_NOINPLACE 32
+
+#define UTL_BLOCK_SIZE 128
+
+/* ==================== per-call drop-in (host buffers) ==================== */
+
+/* PackUint32 (pack.go:76).  Packs n (1..128) values into one block at dst.
+ * Append and NoInPlace only affect where the Go caller places the block and
+ * whether it may reuse values as scratch; the bytes are the same, and the
+ * caller's values are never modified.  dst_cap >= utl_max_block_length32
+ * (flag) always suffices; *out_len receives the block length. */
+UTL_API int utl_pack_u32(uint8_t flag, const uint32_t *values, int n, uint8_t *dst,
+                 size_t dst_cap, size_t *out_len);
+
+/* UnpackUint32 (unpack.go:5).  values must hold 128 entries; *count values
+ * are valid on success, *consumed is the block's byte length.  On
+ * UTL_ERR_OVERFLOW *overflow_pos is ErrOverflow.Position. */
+UTL_API int utl_unpack_u32(const uint8_t *src, size_t src_len, uint32_t *values,
+                   int *count, size_t *consumed, int *overflow_pos);
+
+/* GetUint32 (get.go:74). */
+UTL_API int utl_get_u32(int pos, const uint8_t *src, size_t src_len, uint32_t *value,
+                int *overflow_pos);
+
+/* PackUint64 (uint64.go:279), UnpackUint64 (uint64.go:338),
+ * GetUint64 (uint64.go:364).  dst_cap >= utl_max_block_length64(flag). */
+UTL_API int utl_pack_u64(uint8_t flag, const uint64_t *values, int n, uint8_t *dst,
+                 size_t dst_cap, size_t *out_len);
+UTL_API int utl_unpack_u64(const uint8_t *src, size_t src_len, uint64_t *values,
+                   int *count, size_t *consumed, int *overflow_pos);
+UTL_API int utl_get_u64(int pos, const uint8_t *src, size_t src_len, uint64_t *value,
+                int *overflow_pos);
+
+/* BlockLength (block_length.go:8). */
+UTL_API int utl_block_length(const uint8_t *src, size_t src_len, size_t *block_len);
+
+/* Header (header.go:135); boolean outputs are 0/1. */
+UTL_API int utl_header(const uint8_t *src, size_t src_len, int *count, int *bit_width,
+               int *exc_count, int *has_delta, int *has_for, int *has_zigzag,
+               int *has_special);
+
+/* MaxBlockLength32 (scalar.go:336), MaxBlockLength64 (uint64.go:451). */
+UTL_API int utl_max_block_length32(uint8_t flag);
+UTL_API int utl_max_block_length64(uint8_t flag);
+
+/* Compressor32/Compressor64 (compressor.go:16-107): a handle owning its own
+ * CUDA stream and staging buffers; not safe for concurrent use, like the
+ * reference's type.  is64 selects the 64-bit entry points below. */
+typedef struct utl_codec utl_codec;
+UTL_API int utl_codec_new(int is64, utl_codec **out);
+UTL_API void utl_codec_free(utl_codec *c);
+UTL_API int utl_codec_pack_u32(utl_codec *c, uint8_t flag, const uint32_t *values,
+                       int n, uint8_t *dst, size_t dst_cap, size_t *out_len);
+UTL_API int utl_codec_unpack_u32(utl_codec *c, const uint8_t *src, size_t src_len,
+                         uint32_t *values, int *count, size_t *consumed,
+                         int *overflow_pos);
+UTL_API int utl_codec_get_u32(utl_codec *c, int pos, const uint8_t *src,
+                      size_t src_len, uint32_t *value, int *overflow_pos);
+UTL_API int utl_codec_pack_u64(utl_codec *c, uint8_t flag, const uint64_t *values,
+                       int n, uint8_t *dst, size_t dst_cap, size_t *out_len);
+UTL_API int utl_codec_unpack_u64(utl_codec *c, const uint8_t *src, size_t src_len,
+                         uint64_t *values, int *count, size_t *consumed,
+                         int *overflow_pos);
+UTL_API int utl_codec_get_u64(utl_codec *c, int pos, const uint8_t *src,
+                      size_t src_len, uint64_t *value, int *overflow_pos);
+
+/* ==================== batched (device buffers) ==================== */
+/* One launch packs, unpacks or queries the blocks of many streams of
+ * uneven length.  The reference has no batched form; these replace the
+ * caller's loop of Append / BlockLength-walk calls (example_test.go:171-186)
+ * with one device-wide pass whose block offsets come from an exclusive scan
+ * of the block lengths. */
+
+/* Total blocks of a stream table given on the host (val_off: n_streams+1). */
+UTL_API int64_t utl_count_blocks(const uint64_t *h_val_off, int n_streams);
+
+/* block_start[s] = sum over t<s of ceil(n_t/128), s = 0..n_streams. */
+UTL_API int utl_batch_plan(const uint64_t *d_val_off, int n_streams,
+                   uint64_t *d_block_start, void *stream);
+
+/* Device scratch the pack needs for n_blocks blocks (tile states of the
+ * single-pass offset scan). */
+UTL_API size_t utl_pack_scratch_bytes(int64_t n_blocks);
+
+/* Pack every block of every stream.  d_block_off (n_blocks+1) receives each
+ * block's byte offset in d_out and the total at [n_blocks];
+ * d_stream_byte_off (n_streams+1, optional) each stream's start.
+ * d_err (optional, one uint32, zero it first) receives UTL_ERR_CAPACITY
+ * or UTL_ERR_TIMEOUT bits (1<<code) for the host to check after the stream
+ * synchronizes.  out_cap >= n_blocks*utl_max_block_length32(flag) always
+ * suffices. */
+UTL_API int utl_pack_batch_u32(uint8_t flag, const uint32_t *d_values,
+                       const uint64_t *d_val_off, const uint64_t *d_block_start,
+                       int n_streams, int64_t n_blocks, uint8_t *d_out,
+                       size_t out_cap, uint64_t *d_block_off,
+                       uint64_t *d_stream_byte_off, void *d_scratch,
+                       size_t scratch_bytes, uint32_t *d_err, void *stream);
+UTL_API int utl_pack_batch_u64(uint8_t flag, const uint64_t *d_values,
+                       const uint64_t *d_val_off, const uint64_t *d_block_start,
+                       int n_streams, int64_t n_blocks, uint8_t *d_out,
+                       size_t out_cap, uint64_t *d_block_off,
+                       uint64_t *d_stream_byte_off, void *d_scratch,
+                       size_t scratch_bytes, uint32_t *d_err, void *stream);
+
+/* Unpack every block.  Block b is d_packed[d_block_off[b] .. d_block_off[b+1])
+ * and must decode to the stream table's count, consuming exactly its
+ * length.  d_block_status (optional, n_blocks int32) receives per block
+ * code | (overflow_pos << 8); d_err (optional) gets 1<<code for every code
+ * seen.  Blocks that fail write no values. */
+UTL_API int utl_unpack_batch_u32(const uint8_t *d_packed, size_t packed_len,
+                         const uint64_t *d_block_off, const uint64_t *d_val_off,
+                         const uint64_t *d_block_start, int n_streams,
+                         int64_t n_blocks, uint32_t *d_values,
+                         int32_t *d_block_status, uint32_t *d_err,
+                         void *stream);
+UTL_API int utl_unpack_batch_u64(const uint8_t *d_packed, size_t packed_len,
+                         const uint64_t *d_block_off, const uint64_t *d_val_off,
+                         const uint64_t *d_block_start, int n_streams,
+                         int64_t n_blocks, uint64_t *d_values,
+                         int32_t *d_block_status, uint32_t *d_err,
+                         void *stream);
+
+/* GetUint32/GetUint64 for n_queries (stream, position-in-stream) pairs.
+ * d_status (optional) as for unpack, per query. */
+UTL_API int utl_get_batch_u32(const uint8_t *d_packed, size_t packed_len,
+                      const uint64_t *d_block_off, const uint64_t *d_val_off,
+                      const uint64_t *d_block_start, int n_streams,
+                      const uint32_t *d_q_stream, const uint64_t *d_q_pos,
+                      int64_t n_queries, uint32_t *d_out, int32_t *d_status,
+                      uint32_t *d_err, void *stream);
+UTL_API int utl_get_batch_u64(const uint8_t *d_packed, size_t packed_len,
+                      const uint64_t *d_block_off, const uint64_t *d_val_off,
+                      const uint64_t *d_block_start, int n_streams,
+                      const uint32_t *d_q_stream, const uint64_t *d_q_pos,
+                      int64_t n_queries, uint64_t *d_out, int32_t *d_status,
+                      uint32_t *d_err, void *stream);
+
+/* ==================== batched (host buffers) ==================== */
+/* Same batches end to end from host memory: copies in, one batched pass,
+ * copies out, on the calling thread's context.  Pinned host buffers give
+ * full PCIe bandwidth.  *out_len receives the packed size; h_block_off
+ * (n_blocks+1) and h_stream_byte_off (n_streams+1, optional) as above. */
+UTL_API int utl_pack_streams_u32(uint8_t flag, const uint32_t *h_values,
+                         const uint64_t *h_val_off, int n_streams,
+                         uint8_t *h_out, size_t out_cap, uint64_t *h_block_off,
+                         uint64_t *h_stream_byte_off, size_t *out_len);
+UTL_API int utl_unpack_streams_u32(const uint8_t *h_packed, size_t packed_len,
+                           const uint64_t *h_block_off,
+                           const uint64_t *h_val_off, int n_streams,
+                           uint32_t *h_values);
+UTL_API int utl_pack_streams_u64(uint8_t flag, const uint64_t *h_values,
+                         const uint64_t *h_val_off, int n_streams,
+                         uint8_t *h_out, size_t out_cap, uint64_t *h_block_off,
+                         uint64_t *h_stream_byte_off, size_t *out_len);
+UTL_API int utl_unpack_streams_u64(const uint8_t *h_packed, size_t packed_len,
+                           const uint64_t *h_block_off,
+                           const uint64_t *h_val_off, int n_streams,
+                           uint64_t *h_values);
+
+/* ==================== diagnostics ==================== */
+/* Number of this library's kernels launched so far in this process. */
+UTL_API uint64_t utl_launch_count(void);
+/* Last CUDA error seen by this thread's calls (cudaError_t value). */
+UTL_API int utl_last_cuda_error(void);
+/* Library version string. */
+UTL_API const char *utl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UTLPFOR_H */

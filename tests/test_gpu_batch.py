@@ -1,0 +1,166 @@
+"""GPU parity of the batched device path against the oracle: one launch
+packs many uneven streams byte-identically to block-by-block Append calls,
+unpacks them, and answers Get queries; plus large-size properties."""
+import numpy as np
+import pytest
+
+import oracle_ref as O
+from gen import streams
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+
+    import utlpfor_b200 as U
+    assert torch.cuda.is_available()
+    return U, torch
+
+
+def to_dev(torch, a):
+    a = np.ascontiguousarray(a)
+    return torch.from_numpy(a.view(np.int64 if a.dtype.itemsize == 8 else np.int32)).cuda()
+
+
+LENS = [1, 128, 300, 0, 257, 1000, 5, 129, 0, 4096, 77]
+
+
+@pytest.mark.parametrize("flag", range(8))
+@pytest.mark.parametrize("kind", ["small", "exc", "dense_exc", "sorted", "walk", "wide", "const"])
+def test_pack_unpack_batch_u32(env, flag, kind):
+    U, torch = env
+    rng = np.random.default_rng(flag * 31 + len(kind))
+    vals, vo = streams(rng, LENS, kind)
+    want, wbo, wso = O.pack_streams(flag, vals, vo)
+    pb = U.pack_batch(to_dev(torch, vals), vo, flag)
+    got_len = pb.packed_len
+    assert got_len == len(want)
+    assert np.array_equal(pb.packed[:got_len].cpu().numpy(), want)
+    assert np.array_equal(pb.block_off.cpu().numpy().view(np.uint64), wbo)
+    assert np.array_equal(pb.stream_byte_off.cpu().numpy().view(np.uint64), wso)
+    out = U.unpack_batch(pb)
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), vals)
+
+
+@pytest.mark.parametrize("flag", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("kind", ["for64", "full", "walk", "fit32", "upper_for"])
+def test_pack_unpack_batch_u64(env, flag, kind):
+    U, torch = env
+    rng = np.random.default_rng(500 + flag)
+    vals, vo = streams(rng, LENS, kind, is64=True)
+    want, wbo, wso = O.pack_streams(flag, vals, vo)
+    pb = U.pack_batch(to_dev(torch, vals), vo, flag)
+    assert pb.packed_len == len(want)
+    assert np.array_equal(pb.packed[:pb.packed_len].cpu().numpy(), want)
+    assert np.array_equal(pb.block_off.cpu().numpy().view(np.uint64), wbo)
+    # unpack goes through the reference's decode rules, including its
+    # reading of two-block upper halves with a 4-byte FOR base
+    ref, err = O.unpack_streams(want, wbo, vo, dtype=np.uint64)
+    status = torch.empty(pb.n_blocks, dtype=torch.int32, device="cuda")
+    out = U.unpack_batch(pb, block_status=status, check=False)
+    st = status.cpu().numpy()
+    for s in range(len(LENS)):
+        b0 = int(pb.block_start[s].item())
+        for j in range((LENS[s] + 127) // 128):
+            blk = want[int(wbo[b0 + j]):int(wbo[b0 + j + 1])]
+            ov, oc, oerr, oovf = O.unpack_u64(blk)
+            if oerr == 0 and (len(ov) != min(128, LENS[s] - 128 * j) or oc != len(blk)):
+                oerr = 8
+            assert st[b0 + j] & 0xFF == oerr, (s, j)
+            if oerr == 0:
+                lo = int(vo[s]) + 128 * j
+                assert np.array_equal(out[lo:lo + len(ov)].cpu().numpy().view(np.uint64), ov)
+
+
+@pytest.mark.parametrize("is64", [False, True])
+@pytest.mark.parametrize("flag", [0, 1, 3, 5])
+def test_get_batch(env, is64, flag):
+    U, torch = env
+    rng = np.random.default_rng(77 + flag)
+    kinds = ("sorted", "exc", "walk", "full") if not is64 else ("for64", "full", "walk")
+    for kind in kinds:
+        vals, vo = streams(rng, LENS, kind, is64=is64)
+        packed, bo, so = O.pack_streams(flag, vals, vo)
+        pb = U.pack_batch(to_dev(torch, vals), vo, flag)
+        ns = len(LENS)
+        qs = rng.integers(0, ns + 1, 3000).astype(np.uint32)  # includes an out-of-range stream
+        lens = np.array(LENS + [0])
+        qp = (rng.random(3000) * (lens[qs] + 3)).astype(np.uint64)  # some past the end
+        out, st = U.get_batch(pb, to_dev(torch, qs), to_dev(torch, qp))
+        out = out.cpu().numpy().view(np.uint64 if is64 else np.uint32)
+        st = st.cpu().numpy()
+        for i in range(3000):
+            s, p = int(qs[i]), int(qp[i])
+            if s >= ns or p >= LENS[s]:
+                assert st[i] & 0xFF == 2
+                continue
+            b = int(pb.block_start[s].item()) + p // 128
+            blk = packed[int(bo[b]):int(bo[b + 1])]
+            gv, gerr, govf = (O.get_u64 if is64 else O.get_u32)(p % 128, blk)
+            assert (st[i] & 0xFF, st[i] >> 8) == (gerr, govf)
+            if gerr == 0:
+                assert out[i] == gv == vals[int(vo[s]) + p]
+
+
+def test_unpack_batch_corrupt_blocks(env):
+    """A corrupt block fails its own status only; the others decode."""
+    U, torch = env
+    rng = np.random.default_rng(3)
+    lens = [128 * 40]
+    vals, vo = streams(rng, lens, "exc")
+    packed, bo, _ = O.pack_streams(1, vals, vo)
+    bad = packed.copy()
+    victims = [3, 17, 29]
+    for b in victims:
+        bad[int(bo[b]) + int(rng.integers(0, int(bo[b + 1] - bo[b])))] ^= 0x5A
+    pb = U.pack_batch(to_dev(torch, vals), vo, 1)
+    dev_bad = torch.from_numpy(bad).cuda()
+    status = torch.zeros(pb.n_blocks, dtype=torch.int32, device="cuda")
+    out = U.unpack_batch(pb, block_status=status, check=False, packed=dev_bad)
+    st = status.cpu().numpy()
+    outv = out.cpu().numpy().view(np.uint32)
+    for b in range(pb.n_blocks):
+        blk = bad[int(bo[b]):int(bo[b + 1])]
+        ov, oc, oerr, oovf = O.unpack_u32(blk)
+        if oerr == 0 and (len(ov) != 128 or oc != len(blk)):
+            oerr = 8
+        assert (st[b] & 0xFF, st[b] >> 8) == (oerr, oovf), b
+        if oerr == 0:
+            assert np.array_equal(outv[128 * b:128 * b + 128], ov)
+
+
+def test_host_buffer_streams(env):
+    U, torch = env
+    rng = np.random.default_rng(12)
+    for is64, kind in ((False, "exc"), (True, "walk")):
+        vals, vo = streams(rng, LENS, kind, is64=is64)
+        want, wbo, wso = O.pack_streams(1, vals, vo)
+        packed, bo, so = U.pack_streams(1, vals, vo)
+        assert packed.tobytes() == want.tobytes()
+        assert np.array_equal(bo, wbo) and np.array_equal(so, wso)
+        out = U.unpack_streams(packed, bo, vo, is64=is64)
+        assert np.array_equal(out, vals)
+
+
+def test_large_round_trip_properties(env):
+    """2^24 values with the exception-heavy shape: pack is byte-identical to
+    the oracle (checked by digest), unpack restores every value."""
+    U, torch = env
+    import hashlib
+    rng = np.random.default_rng(2024)
+    n = 1 << 24
+    v = rng.integers(0, 2**8, n, dtype=np.uint64)
+    m = rng.random(n) < 0.02
+    v[m] = rng.integers(2**8, 2**32, int(m.sum()), dtype=np.uint64)
+    v = v.astype(np.uint32)
+    v[: 128 * 1000] = 7  # some all-equal blocks
+    vo = np.array([0, n], dtype=np.uint64)
+    want, wbo, _ = O.pack_streams(0, v, vo, n_threads=8)
+    pb = U.pack_batch(to_dev(torch, v), vo, 0)
+    assert pb.packed_len == len(want)
+    got = pb.packed[:pb.packed_len].cpu().numpy()
+    assert hashlib.sha256(got.tobytes()).digest() == hashlib.sha256(want.tobytes()).digest()
+    out = U.unpack_batch(pb)
+    assert torch.equal(out, to_dev(torch, v))

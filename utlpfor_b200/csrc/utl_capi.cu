@@ -1,0 +1,659 @@
+// utl_capi.cu -- C ABI of the UTL-PFOR codec (declared in include/utlpfor.h).
+//
+// Per-call entry points run one single-warp kernel per call.  Inputs are
+// copied into a mapped, pinned staging buffer that the kernel reads over
+// PCIe, and the kernel writes its result record and output back into the
+// same buffer, so a call costs one launch and one stream synchronize.
+// Each host thread owns one context (stream + staging) per device; a
+// utl_codec handle owns its own.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <unordered_map>
+
+#include "../../include/utlpfor.h"
+#include "utl_launch.h"
+
+namespace utl {
+
+static std::atomic<uint64_t> g_launches{0};
+void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
+
+static thread_local int t_last_cuda = 0;
+
+static int cuda_fail(cudaError_t e) {
+  t_last_cuda = (int)e;
+  return UTL_ERR_CUDA;
+}
+#define UTL_CUDA(x)                          \
+  do {                                       \
+    cudaError_t _e = (x);                    \
+    if (_e != cudaSuccess) return cuda_fail(_e); \
+  } while (0)
+
+static inline uint32_t ld16(const uint8_t* p) { return (uint32_t)p[0] | ((uint32_t)p[1] << 8); }
+static inline uint32_t ld32(const uint8_t* p) {
+  return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+}
+
+// Staging layout of a context's mapped buffer.
+constexpr size_t kStageIn = 144 * 1024;  // covers the largest span a corrupt block can name
+constexpr size_t kStageOut = 4096;       // one packed block (<= 2038 B) or 128 values
+constexpr size_t kStageRes = 256;
+constexpr size_t kStageBytes = kStageIn + kStageOut + kStageRes;
+
+struct Grow {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max(n, (size_t)256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint8_t* h_stage = nullptr;  // mapped pinned
+  uint8_t* d_stage = nullptr;  // device alias of h_stage
+  uint8_t* d_tmp = nullptr;    // device copy of staged input
+  // buffers of the host-buffer batch path
+  Grow values, val_off, bstart, packed, block_off, sbo, scratch, err;
+
+  int init() {
+    UTL_CUDA(cudaGetDevice(&device));
+    UTL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    UTL_CUDA(cudaHostAlloc((void**)&h_stage, kStageBytes, cudaHostAllocMapped | cudaHostAllocPortable));
+    UTL_CUDA(cudaHostGetDevicePointer((void**)&d_stage, h_stage, 0));
+    UTL_CUDA(cudaMalloc((void**)&d_tmp, kStageIn));
+    return UTL_OK;
+  }
+  void destroy() {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    Grow* gs[] = {&values, &val_off, &bstart, &packed, &block_off, &sbo, &scratch, &err};
+    for (Grow* g : gs) g->release();
+    if (d_tmp) cudaFree(d_tmp);
+    if (h_stage) cudaFreeHost(h_stage);
+    if (stream) cudaStreamDestroy(stream);
+    cudaSetDevice(cur);
+  }
+  uint8_t* in_h() { return h_stage; }
+  uint8_t* in_d() { return d_stage; }
+  uint8_t* out_h() { return h_stage + kStageIn; }
+  uint8_t* out_d() { return d_stage + kStageIn; }
+  PlainResult* res_h() { return (PlainResult*)(h_stage + kStageIn + kStageOut); }
+  PlainResult* res_d() { return (PlainResult*)(d_stage + kStageIn + kStageOut); }
+};
+
+// One context per (host thread, device), released at thread exit.
+struct ThreadCtxs {
+  std::unordered_map<int, Ctx*> m;
+  ~ThreadCtxs() {
+    for (auto& kv : m) {
+      kv.second->destroy();
+      delete kv.second;
+    }
+  }
+};
+static thread_local ThreadCtxs t_ctxs;
+
+static int thread_ctx(Ctx** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e);
+  auto it = t_ctxs.m.find(dev);
+  if (it != t_ctxs.m.end()) {
+    *out = it->second;
+    return UTL_OK;
+  }
+  Ctx* c = new Ctx();
+  int rc = c->init();
+  if (rc != UTL_OK) {
+    c->destroy();
+    delete c;
+    return rc;
+  }
+  t_ctxs.m[dev] = c;
+  *out = c;
+  return UTL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// header helpers (host): block_length.go:8-65, header.go:135-153,
+// scalar.go:336-357, uint64.go:451-453
+// ---------------------------------------------------------------------------
+static int block_length_host(const uint8_t* src, size_t len, size_t* out) {
+  if (!src && len) return UTL_ERR_ARG;
+  if (len < 4) return UTL_ERR_INVALID_BUFFER;
+  const uint32_t h = ld32(src);
+  const int count = (int)(h & 0xFF), bw = (int)((h >> 8) & 31) * 4, itype = (int)((h >> 13) & 3);
+  const int forw = (int)((h >> 15) & 3), exc = (int)(h >> 24);
+  if (count > UTL_BLOCK_SIZE) return UTL_ERR_INVALID_BLOCK_LENGTH;
+  if (bw > 32) return UTL_ERR_INVALID_BUFFER;
+  const bool combine = (h & (1u << 19)) && itype == 3;
+  if (itype == 3) {
+    if (h & ((1u << 18) | (1u << 20))) return UTL_ERR_INVALID_FLAGS;
+  } else if (h & ((1u << 18) | (1u << 19) | (1u << 20))) {
+    return UTL_ERR_INVALID_FLAGS;
+  }
+  const size_t forb = (itype == 3 && !combine && forw == 3) ? 8 : (size_t)((1 << forw) >> 1);
+  const size_t p_off = 4 + (exc ? 2 : 0) + forb + (combine ? 2 : 0);
+  size_t b1 = p_off + ((size_t)bw << 4);
+  if (exc) {
+    if (len < 6) return UTL_ERR_INVALID_BUFFER;
+    b1 += (size_t)(exc <= 16 ? exc : 16) + ld16(src + 4);
+  }
+  if (!combine) {
+    *out = b1;
+    return UTL_OK;
+  }
+  if (len < p_off) return UTL_ERR_INVALID_BUFFER;
+  *out = b1 + ld16(src + p_off - 2);
+  return UTL_OK;
+}
+
+// Upper bound of the bytes a decode of src may touch, from header fields
+// alone (no validation): the per-call kernels stage only this much.
+static size_t staged_extent(const uint8_t* src, size_t len) {
+  if (len < 6) return len;
+  const uint32_t h = ld32(src);
+  const int bw = (int)((h >> 8) & 31) * 4, forw = (int)((h >> 15) & 3), exc = (int)(h >> 24);
+  const bool combine = (h & (1u << 19)) != 0;
+  size_t p_off = 4 + (exc ? 2 : 0) + (forw ? 8 : 0) + (combine ? 2 : 0);
+  size_t e = p_off + (size_t)bw * 16 + (exc ? 16 + ld16(src + 4) : 0);
+  if (combine) {
+    size_t b2 = 4 + (exc ? 2 : 0) + (size_t)((1 << forw) >> 1);
+    if (b2 + 2 <= len) e += ld16(src + b2);
+  }
+  return std::min(len, e + 64);
+}
+
+}  // namespace utl
+
+using namespace utl;
+
+// ---------------------------------------------------------------------------
+// per-call entry points
+// ---------------------------------------------------------------------------
+static int pack_call(Ctx* c, bool u64, uint8_t flag, const void* values, int n, uint8_t* dst, size_t dst_cap,
+                     size_t* out_len) {
+  if (n <= 0 || n > UTL_BLOCK_SIZE) return UTL_ERR_INVALID_BUFFER;  // pack.go / scalar.go:240
+  if (!values || !dst || !out_len) return UTL_ERR_ARG;
+  memcpy(c->in_h(), values, (size_t)n * (u64 ? 8 : 4));
+  c->res_h()->status = -1;
+  cudaError_t e = launch::plain_pack(u64, flag, c->in_d(), n, c->out_d(), c->res_d(), c->stream);
+  if (e != cudaSuccess) return cuda_fail(e);
+  e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e);
+  const PlainResult r = *c->res_h();
+  if (r.status != UTL_OK) return r.status;
+  if ((size_t)r.len > dst_cap) return UTL_ERR_CAPACITY;
+  memcpy(dst, c->out_h(), (size_t)r.len);
+  *out_len = (size_t)r.len;
+  return UTL_OK;
+}
+
+static int unpack_call(Ctx* c, bool u64, const uint8_t* src, size_t src_len, void* values, int* count,
+                       size_t* consumed, int* ovf) {
+  if ((!src && src_len) || !values || !count || !consumed) return UTL_ERR_ARG;
+  const size_t staged = staged_extent(src, src_len);
+  if (staged > kStageIn) return UTL_ERR_ARG;
+  if (staged) memcpy(c->in_h(), src, staged);
+  c->res_h()->status = -1;
+  cudaError_t e = launch::plain_unpack(u64, c->in_d(), (int64_t)staged, (int64_t)src_len, c->d_tmp, c->out_d(),
+                                       c->res_d(), c->stream);
+  if (e != cudaSuccess) return cuda_fail(e);
+  e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e);
+  const PlainResult r = *c->res_h();
+  if (r.status != UTL_OK) {
+    if (r.status == UTL_ERR_OVERFLOW && ovf) *ovf = r.ovf;
+    return r.status;
+  }
+  memcpy(values, c->out_h(), (size_t)r.count * (u64 ? 8 : 4));
+  *count = r.count;
+  *consumed = (size_t)r.len;
+  return UTL_OK;
+}
+
+static int get_call(Ctx* c, bool u64, int pos, const uint8_t* src, size_t src_len, uint64_t* value, int* ovf) {
+  if ((!src && src_len) || !value) return UTL_ERR_ARG;
+  const size_t staged = staged_extent(src, src_len);
+  if (staged > kStageIn) return UTL_ERR_ARG;
+  if (staged) memcpy(c->in_h(), src, staged);
+  c->res_h()->status = -1;
+  cudaError_t e = launch::plain_get(u64, pos, c->in_d(), (int64_t)staged, (int64_t)src_len, c->d_tmp, c->res_d(),
+                                    c->stream);
+  if (e != cudaSuccess) return cuda_fail(e);
+  e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e);
+  const PlainResult r = *c->res_h();
+  if (r.status != UTL_OK) {
+    if (r.status == UTL_ERR_OVERFLOW && ovf) *ovf = r.ovf;
+    return r.status;
+  }
+  *value = r.value;
+  return UTL_OK;
+}
+
+#define WITH_CTX(expr)                 \
+  Ctx* c_ = nullptr;                   \
+  int rc_ = thread_ctx(&c_);           \
+  if (rc_ != UTL_OK) return rc_;       \
+  return (expr)
+
+struct utl_codec {
+  Ctx ctx;
+};
+
+extern "C" {
+
+int utl_pack_u32(uint8_t flag, const uint32_t* values, int n, uint8_t* dst, size_t dst_cap, size_t* out_len) {
+  WITH_CTX(pack_call(c_, false, flag, values, n, dst, dst_cap, out_len));
+}
+int utl_pack_u64(uint8_t flag, const uint64_t* values, int n, uint8_t* dst, size_t dst_cap, size_t* out_len) {
+  WITH_CTX(pack_call(c_, true, flag, values, n, dst, dst_cap, out_len));
+}
+int utl_unpack_u32(const uint8_t* src, size_t src_len, uint32_t* values, int* count, size_t* consumed,
+                   int* overflow_pos) {
+  WITH_CTX(unpack_call(c_, false, src, src_len, values, count, consumed, overflow_pos));
+}
+int utl_unpack_u64(const uint8_t* src, size_t src_len, uint64_t* values, int* count, size_t* consumed,
+                   int* overflow_pos) {
+  WITH_CTX(unpack_call(c_, true, src, src_len, values, count, consumed, overflow_pos));
+}
+int utl_get_u32(int pos, const uint8_t* src, size_t src_len, uint32_t* value, int* overflow_pos) {
+  if (!value) return UTL_ERR_ARG;
+  uint64_t v = 0;
+  Ctx* c = nullptr;
+  int rc = thread_ctx(&c);
+  if (rc != UTL_OK) return rc;
+  rc = get_call(c, false, pos, src, src_len, &v, overflow_pos);
+  if (rc == UTL_OK) *value = (uint32_t)v;
+  return rc;
+}
+int utl_get_u64(int pos, const uint8_t* src, size_t src_len, uint64_t* value, int* overflow_pos) {
+  WITH_CTX(get_call(c_, true, pos, src, src_len, value, overflow_pos));
+}
+
+int utl_block_length(const uint8_t* src, size_t src_len, size_t* block_len) {
+  if (!block_len) return UTL_ERR_ARG;
+  return block_length_host(src, src_len, block_len);
+}
+
+int utl_header(const uint8_t* src, size_t src_len, int* count, int* bit_width, int* exc_count, int* has_delta,
+               int* has_for, int* has_zigzag, int* has_special) {
+  int* outs[] = {count, bit_width, exc_count, has_delta, has_for, has_zigzag, has_special};
+  for (int* o : outs)
+    if (!o) return UTL_ERR_ARG;
+  for (int* o : outs) *o = 0;
+  if (src_len < 4 || !src) return UTL_ERR_INVALID_BUFFER;
+  const uint32_t h = ld32(src);
+  const int itype = (int)((h >> 13) & 3);
+  if (itype != 2 && itype != 1) return UTL_ERR_UNSUPPORTED_TYPE;
+  *count = (int)(h & 0xFF);
+  *bit_width = (int)((h >> 8) & 31) * 4;
+  *exc_count = (int)(h >> 24);
+  *has_delta = (h >> 22) & 1;
+  *has_for = ((h >> 15) & 3) > 0;
+  *has_zigzag = (h >> 23) & 1;
+  *has_special = (h >> 17) & 1;
+  return UTL_OK;
+}
+
+int utl_max_block_length32(uint8_t flag) {
+  const int forb = (flag & UTL_NOFOR) ? 0 : 4;
+  if (flag & UTL_NOPATCH) return 4 + forb + 32 * 16;
+  return 4 + 2 + forb + 28 * 16 + 16 + (32 + 4 * 128);
+}
+int utl_max_block_length64(uint8_t flag) { return 2 * utl_max_block_length32(flag) + 2; }
+
+int utl_codec_new(int is64, utl_codec** out) {
+  (void)is64;
+  if (!out) return UTL_ERR_ARG;
+  utl_codec* c = new utl_codec();
+  int rc = c->ctx.init();
+  if (rc != UTL_OK) {
+    c->ctx.destroy();
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return UTL_OK;
+}
+void utl_codec_free(utl_codec* c) {
+  if (!c) return;
+  c->ctx.destroy();
+  delete c;
+}
+int utl_codec_pack_u32(utl_codec* c, uint8_t flag, const uint32_t* values, int n, uint8_t* dst, size_t dst_cap,
+                       size_t* out_len) {
+  if (!c) return UTL_ERR_ARG;
+  return pack_call(&c->ctx, false, flag, values, n, dst, dst_cap, out_len);
+}
+int utl_codec_unpack_u32(utl_codec* c, const uint8_t* src, size_t src_len, uint32_t* values, int* count,
+                         size_t* consumed, int* overflow_pos) {
+  if (!c) return UTL_ERR_ARG;
+  return unpack_call(&c->ctx, false, src, src_len, values, count, consumed, overflow_pos);
+}
+int utl_codec_get_u32(utl_codec* c, int pos, const uint8_t* src, size_t src_len, uint32_t* value, int* overflow_pos) {
+  if (!c || !value) return UTL_ERR_ARG;
+  uint64_t v = 0;
+  int rc = get_call(&c->ctx, false, pos, src, src_len, &v, overflow_pos);
+  if (rc == UTL_OK) *value = (uint32_t)v;
+  return rc;
+}
+int utl_codec_pack_u64(utl_codec* c, uint8_t flag, const uint64_t* values, int n, uint8_t* dst, size_t dst_cap,
+                       size_t* out_len) {
+  if (!c) return UTL_ERR_ARG;
+  return pack_call(&c->ctx, true, flag, values, n, dst, dst_cap, out_len);
+}
+int utl_codec_unpack_u64(utl_codec* c, const uint8_t* src, size_t src_len, uint64_t* values, int* count,
+                         size_t* consumed, int* overflow_pos) {
+  if (!c) return UTL_ERR_ARG;
+  return unpack_call(&c->ctx, true, src, src_len, values, count, consumed, overflow_pos);
+}
+int utl_codec_get_u64(utl_codec* c, int pos, const uint8_t* src, size_t src_len, uint64_t* value, int* overflow_pos) {
+  if (!c) return UTL_ERR_ARG;
+  return get_call(&c->ctx, true, pos, src, src_len, value, overflow_pos);
+}
+
+// ---------------------------------------------------------------------------
+// batched, device buffers
+// ---------------------------------------------------------------------------
+int64_t utl_count_blocks(const uint64_t* h_val_off, int n_streams) {
+  if (!h_val_off || n_streams < 0) return -1;
+  int64_t nb = 0;
+  for (int s = 0; s < n_streams; s++) {
+    if (h_val_off[s + 1] < h_val_off[s]) return -1;
+    nb += (int64_t)((h_val_off[s + 1] - h_val_off[s] + UTL_BLOCK_SIZE - 1) / UTL_BLOCK_SIZE);
+  }
+  return nb;
+}
+
+int utl_batch_plan(const uint64_t* d_val_off, int n_streams, uint64_t* d_block_start, void* stream) {
+  if (!d_val_off || !d_block_start || n_streams < 0) return UTL_ERR_ARG;
+  cudaError_t e = launch::plan(d_val_off, n_streams, d_block_start, (cudaStream_t)stream);
+  return e == cudaSuccess ? UTL_OK : cuda_fail(e);
+}
+
+size_t utl_pack_scratch_bytes(int64_t n_blocks) { return launch::pack_scratch_bytes(n_blocks < 0 ? 0 : n_blocks); }
+
+static int pack_batch(bool u64, uint8_t flag, const void* d_values, const uint64_t* d_val_off,
+                      const uint64_t* d_block_start, int n_streams, int64_t n_blocks, uint8_t* d_out, size_t out_cap,
+                      uint64_t* d_block_off, uint64_t* d_sbo, void* d_scratch, size_t scratch_bytes, uint32_t* d_err,
+                      cudaStream_t st) {
+  if (n_streams < 0 || n_blocks < 0 || !d_val_off || !d_block_start || !d_block_off) return UTL_ERR_ARG;
+  if (n_blocks > 0 && (!d_values || !d_out || !d_scratch)) return UTL_ERR_ARG;
+  if (((uintptr_t)d_out & 3) != 0) return UTL_ERR_ARG;
+  if (n_blocks == 0) {
+    UTL_CUDA(cudaMemsetAsync(d_block_off, 0, sizeof(uint64_t), st));
+  } else {
+    if (scratch_bytes < launch::pack_scratch_bytes(n_blocks)) return UTL_ERR_ARG;
+    UTL_CUDA(cudaMemsetAsync(d_scratch, 0, launch::pack_scratch_bytes(n_blocks), st));
+    PackArgs a;
+    a.values = d_values;
+    a.val_off = d_val_off;
+    a.block_start = d_block_start;
+    a.n_streams = n_streams;
+    a.flag = flag;
+    a.n_blocks = n_blocks;
+    a.n_tiles = launch::tiles_for(n_blocks);
+    a.out = d_out;
+    a.out_cap = out_cap;
+    a.block_off = d_block_off;
+    a.counter = (unsigned long long*)d_scratch;
+    a.tile_status = (uint64_t*)((uint8_t*)d_scratch + 16);
+    a.err = d_err;
+    cudaError_t e = launch::pack(u64, a, st);
+    if (e != cudaSuccess) return cuda_fail(e);
+  }
+  if (d_sbo) {
+    cudaError_t e = launch::stream_offsets(d_block_off, d_block_start, n_streams, d_sbo, st);
+    if (e != cudaSuccess) return cuda_fail(e);
+  }
+  return UTL_OK;
+}
+
+int utl_pack_batch_u32(uint8_t flag, const uint32_t* d_values, const uint64_t* d_val_off,
+                       const uint64_t* d_block_start, int n_streams, int64_t n_blocks, uint8_t* d_out, size_t out_cap,
+                       uint64_t* d_block_off, uint64_t* d_stream_byte_off, void* d_scratch, size_t scratch_bytes,
+                       uint32_t* d_err, void* stream) {
+  return pack_batch(false, flag, d_values, d_val_off, d_block_start, n_streams, n_blocks, d_out, out_cap, d_block_off,
+                    d_stream_byte_off, d_scratch, scratch_bytes, d_err, (cudaStream_t)stream);
+}
+int utl_pack_batch_u64(uint8_t flag, const uint64_t* d_values, const uint64_t* d_val_off,
+                       const uint64_t* d_block_start, int n_streams, int64_t n_blocks, uint8_t* d_out, size_t out_cap,
+                       uint64_t* d_block_off, uint64_t* d_stream_byte_off, void* d_scratch, size_t scratch_bytes,
+                       uint32_t* d_err, void* stream) {
+  return pack_batch(true, flag, d_values, d_val_off, d_block_start, n_streams, n_blocks, d_out, out_cap, d_block_off,
+                    d_stream_byte_off, d_scratch, scratch_bytes, d_err, (cudaStream_t)stream);
+}
+
+static int unpack_batch(bool u64, const uint8_t* d_packed, size_t packed_len, const uint64_t* d_block_off,
+                        const uint64_t* d_val_off, const uint64_t* d_block_start, int n_streams, int64_t n_blocks,
+                        void* d_values, int32_t* d_status, uint32_t* d_err, cudaStream_t st) {
+  if (n_streams < 0 || n_blocks < 0) return UTL_ERR_ARG;
+  if (n_blocks == 0) return UTL_OK;
+  if (!d_packed || !d_block_off || !d_val_off || !d_block_start || !d_values) return UTL_ERR_ARG;
+  UnpackArgs a;
+  a.packed = d_packed;
+  a.packed_len = packed_len;
+  a.block_off = d_block_off;
+  a.val_off = d_val_off;
+  a.block_start = d_block_start;
+  a.n_streams = n_streams;
+  a.n_blocks = n_blocks;
+  a.values = d_values;
+  a.block_status = d_status;
+  a.err = d_err;
+  cudaError_t e = launch::unpack(u64, a, st);
+  return e == cudaSuccess ? UTL_OK : cuda_fail(e);
+}
+
+int utl_unpack_batch_u32(const uint8_t* d_packed, size_t packed_len, const uint64_t* d_block_off,
+                         const uint64_t* d_val_off, const uint64_t* d_block_start, int n_streams, int64_t n_blocks,
+                         uint32_t* d_values, int32_t* d_block_status, uint32_t* d_err, void* stream) {
+  return unpack_batch(false, d_packed, packed_len, d_block_off, d_val_off, d_block_start, n_streams, n_blocks,
+                      d_values, d_block_status, d_err, (cudaStream_t)stream);
+}
+int utl_unpack_batch_u64(const uint8_t* d_packed, size_t packed_len, const uint64_t* d_block_off,
+                         const uint64_t* d_val_off, const uint64_t* d_block_start, int n_streams, int64_t n_blocks,
+                         uint64_t* d_values, int32_t* d_block_status, uint32_t* d_err, void* stream) {
+  return unpack_batch(true, d_packed, packed_len, d_block_off, d_val_off, d_block_start, n_streams, n_blocks,
+                      d_values, d_block_status, d_err, (cudaStream_t)stream);
+}
+
+static int get_batch(bool u64, const uint8_t* d_packed, size_t packed_len, const uint64_t* d_block_off,
+                     const uint64_t* d_val_off, const uint64_t* d_block_start, int n_streams,
+                     const uint32_t* d_q_stream, const uint64_t* d_q_pos, int64_t n_queries, void* d_out,
+                     int32_t* d_status, uint32_t* d_err, cudaStream_t st) {
+  if (n_queries < 0 || n_streams < 0) return UTL_ERR_ARG;
+  if (n_queries == 0) return UTL_OK;
+  if (!d_block_off || !d_val_off || !d_block_start || !d_q_stream || !d_q_pos || !d_out) return UTL_ERR_ARG;
+  GetArgs a;
+  a.packed = d_packed;
+  a.packed_len = packed_len;
+  a.block_off = d_block_off;
+  a.val_off = d_val_off;
+  a.block_start = d_block_start;
+  a.n_streams = n_streams;
+  a.q_stream = d_q_stream;
+  a.q_pos = d_q_pos;
+  a.n_queries = n_queries;
+  a.out = d_out;
+  a.status = d_status;
+  a.err = d_err;
+  cudaError_t e = launch::get(u64, a, st);
+  return e == cudaSuccess ? UTL_OK : cuda_fail(e);
+}
+
+int utl_get_batch_u32(const uint8_t* d_packed, size_t packed_len, const uint64_t* d_block_off,
+                      const uint64_t* d_val_off, const uint64_t* d_block_start, int n_streams,
+                      const uint32_t* d_q_stream, const uint64_t* d_q_pos, int64_t n_queries, uint32_t* d_out,
+                      int32_t* d_status, uint32_t* d_err, void* stream) {
+  return get_batch(false, d_packed, packed_len, d_block_off, d_val_off, d_block_start, n_streams, d_q_stream, d_q_pos,
+                   n_queries, d_out, d_status, d_err, (cudaStream_t)stream);
+}
+int utl_get_batch_u64(const uint8_t* d_packed, size_t packed_len, const uint64_t* d_block_off,
+                      const uint64_t* d_val_off, const uint64_t* d_block_start, int n_streams,
+                      const uint32_t* d_q_stream, const uint64_t* d_q_pos, int64_t n_queries, uint64_t* d_out,
+                      int32_t* d_status, uint32_t* d_err, void* stream) {
+  return get_batch(true, d_packed, packed_len, d_block_off, d_val_off, d_block_start, n_streams, d_q_stream, d_q_pos,
+                   n_queries, d_out, d_status, d_err, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------
+// batched, host buffers
+// ---------------------------------------------------------------------------
+static int first_error(uint32_t bits) {
+  for (int c = 1; c < 32; c++)
+    if (bits & (1u << c)) return c;
+  return UTL_OK;
+}
+
+static int pack_streams(bool u64, uint8_t flag, const void* h_values, const uint64_t* h_val_off, int n_streams,
+                        uint8_t* h_out, size_t out_cap, uint64_t* h_block_off, uint64_t* h_sbo, size_t* out_len) {
+  if (!h_val_off || n_streams < 0 || !out_len || !h_block_off) return UTL_ERR_ARG;
+  const int64_t nb = utl_count_blocks(h_val_off, n_streams);
+  if (nb < 0) return UTL_ERR_ARG;
+  Ctx* c = nullptr;
+  int rc = thread_ctx(&c);
+  if (rc != UTL_OK) return rc;
+  const size_t esz = u64 ? 8 : 4;
+  const uint64_t v0 = h_val_off[0], nv = h_val_off[n_streams] - v0;
+  const size_t maxb = (size_t)(u64 ? utl_max_block_length64(flag) : utl_max_block_length32(flag));
+  UTL_CUDA(c->values.ensure(nv * esz));
+  UTL_CUDA(c->val_off.ensure(((size_t)n_streams + 1) * 8));
+  UTL_CUDA(c->bstart.ensure(((size_t)n_streams + 1) * 8));
+  UTL_CUDA(c->packed.ensure((size_t)nb * maxb + 16));
+  UTL_CUDA(c->block_off.ensure(((size_t)nb + 1) * 8));
+  UTL_CUDA(c->sbo.ensure(((size_t)n_streams + 1) * 8));
+  UTL_CUDA(c->scratch.ensure(launch::pack_scratch_bytes(nb)));
+  UTL_CUDA(c->err.ensure(8));
+  cudaStream_t st = c->stream;
+  if (nv) UTL_CUDA(cudaMemcpyAsync(c->values.p, (const uint8_t*)h_values + v0 * esz, nv * esz, cudaMemcpyHostToDevice, st));
+  UTL_CUDA(cudaMemsetAsync(c->err.p, 0, 4, st));
+  // value offsets are rebased to the copied range when the table does not start at zero
+  uint64_t* dvo = (uint64_t*)c->val_off.p;
+  if (v0) {
+    uint64_t* tmp = new uint64_t[(size_t)n_streams + 1];
+    for (int s = 0; s <= n_streams; s++) tmp[s] = h_val_off[s] - v0;
+    cudaError_t e = cudaMemcpyAsync(dvo, tmp, ((size_t)n_streams + 1) * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    delete[] tmp;
+    if (e != cudaSuccess) return cuda_fail(e);
+  } else {
+    UTL_CUDA(cudaMemcpyAsync(dvo, h_val_off, ((size_t)n_streams + 1) * 8, cudaMemcpyHostToDevice, st));
+  }
+  cudaError_t e = launch::plan(dvo, n_streams, (uint64_t*)c->bstart.p, st);
+  if (e != cudaSuccess) return cuda_fail(e);
+  rc = pack_batch(u64, flag, c->values.p, dvo, (const uint64_t*)c->bstart.p, n_streams, nb, (uint8_t*)c->packed.p,
+                  c->packed.cap, (uint64_t*)c->block_off.p, h_sbo ? (uint64_t*)c->sbo.p : nullptr, c->scratch.p,
+                  c->scratch.cap, (uint32_t*)c->err.p, st);
+  if (rc != UTL_OK) return rc;
+  UTL_CUDA(cudaMemcpyAsync(h_block_off, c->block_off.p, ((size_t)nb + 1) * 8, cudaMemcpyDeviceToHost, st));
+  uint32_t errbits = 0;
+  UTL_CUDA(cudaMemcpyAsync(&errbits, c->err.p, 4, cudaMemcpyDeviceToHost, st));
+  if (h_sbo) UTL_CUDA(cudaMemcpyAsync(h_sbo, c->sbo.p, ((size_t)n_streams + 1) * 8, cudaMemcpyDeviceToHost, st));
+  UTL_CUDA(cudaStreamSynchronize(st));
+  if (errbits) return first_error(errbits);
+  const size_t total = (size_t)h_block_off[nb];
+  *out_len = total;
+  if (total > out_cap || (total && !h_out)) return UTL_ERR_CAPACITY;
+  if (total) {
+    UTL_CUDA(cudaMemcpyAsync(h_out, c->packed.p, total, cudaMemcpyDeviceToHost, st));
+    UTL_CUDA(cudaStreamSynchronize(st));
+  }
+  return UTL_OK;
+}
+
+static int unpack_streams(bool u64, const uint8_t* h_packed, size_t packed_len, const uint64_t* h_block_off,
+                          const uint64_t* h_val_off, int n_streams, void* h_values) {
+  if (!h_val_off || !h_block_off || n_streams < 0) return UTL_ERR_ARG;
+  const int64_t nb = utl_count_blocks(h_val_off, n_streams);
+  if (nb < 0) return UTL_ERR_ARG;
+  if (nb == 0) return UTL_OK;
+  if (!h_packed || !h_values) return UTL_ERR_ARG;
+  Ctx* c = nullptr;
+  int rc = thread_ctx(&c);
+  if (rc != UTL_OK) return rc;
+  const size_t esz = u64 ? 8 : 4;
+  const uint64_t v0 = h_val_off[0], nv = h_val_off[n_streams] - v0;
+  UTL_CUDA(c->values.ensure(nv * esz));
+  UTL_CUDA(c->val_off.ensure(((size_t)n_streams + 1) * 8));
+  UTL_CUDA(c->bstart.ensure(((size_t)n_streams + 1) * 8));
+  UTL_CUDA(c->packed.ensure(packed_len + 16));
+  UTL_CUDA(c->block_off.ensure(((size_t)nb + 1) * 8));
+  UTL_CUDA(c->err.ensure(8));
+  cudaStream_t st = c->stream;
+  UTL_CUDA(cudaMemcpyAsync(c->packed.p, h_packed, packed_len, cudaMemcpyHostToDevice, st));
+  UTL_CUDA(cudaMemcpyAsync(c->block_off.p, h_block_off, ((size_t)nb + 1) * 8, cudaMemcpyHostToDevice, st));
+  UTL_CUDA(cudaMemsetAsync(c->err.p, 0, 4, st));
+  uint64_t* dvo = (uint64_t*)c->val_off.p;
+  if (v0) {
+    uint64_t* tmp = new uint64_t[(size_t)n_streams + 1];
+    for (int s = 0; s <= n_streams; s++) tmp[s] = h_val_off[s] - v0;
+    cudaError_t e = cudaMemcpyAsync(dvo, tmp, ((size_t)n_streams + 1) * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    delete[] tmp;
+    if (e != cudaSuccess) return cuda_fail(e);
+  } else {
+    UTL_CUDA(cudaMemcpyAsync(dvo, h_val_off, ((size_t)n_streams + 1) * 8, cudaMemcpyHostToDevice, st));
+  }
+  cudaError_t e = launch::plan(dvo, n_streams, (uint64_t*)c->bstart.p, st);
+  if (e != cudaSuccess) return cuda_fail(e);
+  rc = unpack_batch(u64, (const uint8_t*)c->packed.p, packed_len, (const uint64_t*)c->block_off.p, dvo,
+                    (const uint64_t*)c->bstart.p, n_streams, nb, c->values.p, nullptr, (uint32_t*)c->err.p, st);
+  if (rc != UTL_OK) return rc;
+  uint32_t errbits = 0;
+  UTL_CUDA(cudaMemcpyAsync(&errbits, c->err.p, 4, cudaMemcpyDeviceToHost, st));
+  UTL_CUDA(cudaMemcpyAsync((uint8_t*)h_values + v0 * esz, c->values.p, nv * esz, cudaMemcpyDeviceToHost, st));
+  UTL_CUDA(cudaStreamSynchronize(st));
+  return errbits ? first_error(errbits) : UTL_OK;
+}
+
+int utl_pack_streams_u32(uint8_t flag, const uint32_t* h_values, const uint64_t* h_val_off, int n_streams,
+                         uint8_t* h_out, size_t out_cap, uint64_t* h_block_off, uint64_t* h_stream_byte_off,
+                         size_t* out_len) {
+  return pack_streams(false, flag, h_values, h_val_off, n_streams, h_out, out_cap, h_block_off, h_stream_byte_off,
+                      out_len);
+}
+int utl_pack_streams_u64(uint8_t flag, const uint64_t* h_values, const uint64_t* h_val_off, int n_streams,
+                         uint8_t* h_out, size_t out_cap, uint64_t* h_block_off, uint64_t* h_stream_byte_off,
+                         size_t* out_len) {
+  return pack_streams(true, flag, h_values, h_val_off, n_streams, h_out, out_cap, h_block_off, h_stream_byte_off,
+                      out_len);
+}
+int utl_unpack_streams_u32(const uint8_t* h_packed, size_t packed_len, const uint64_t* h_block_off,
+                           const uint64_t* h_val_off, int n_streams, uint32_t* h_values) {
+  return unpack_streams(false, h_packed, packed_len, h_block_off, h_val_off, n_streams, h_values);
+}
+int utl_unpack_streams_u64(const uint8_t* h_packed, size_t packed_len, const uint64_t* h_block_off,
+                           const uint64_t* h_val_off, int n_streams, uint64_t* h_values) {
+  return unpack_streams(true, h_packed, packed_len, h_block_off, h_val_off, n_streams, h_values);
+}
+
+uint64_t utl_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+int utl_last_cuda_error(void) { return t_last_cuda; }
+const char* utl_version(void) { return "utlpfor-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,782 @@
+// utl_kernels.cu -- batched and per-call kernels of the UTL-PFOR codec.
+//
+// Batched pack: a persistent kernel whose CTAs take tiles of kTile blocks
+// from a device work counter.  Each warp packs its blocks into shared-memory
+// slots, warp 0 scans the tile's block lengths and resolves the tile's
+// global byte offset with a decoupled look-back over the tiles before it,
+// and the warps then copy their blocks to HBM at the final offsets: one
+// pass over the values, packed bytes written once, block index written as
+// a by-product.  The result is byte-identical to calling the reference's
+// PackUint32(flag|Append, ...) block after block (pack.go:76-97).
+//
+// Batched unpack: one CTA per tile; the tile's contiguous packed bytes are
+// staged into shared memory with 16-byte loads, then each warp decodes its
+// blocks (warp_unpack_block) and writes 128-byte coalesced rows of values.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "utl_device.cuh"
+#include "utl_launch.h"
+
+namespace utl {
+
+constexpr int kWarps = 8;
+constexpr int kBlocksPerWarp = 2;
+constexpr int kTile = kWarps * kBlocksPerWarp;  // blocks per CTA tile
+constexpr int kThreads = kWarps * 32;
+
+template <bool U64> struct Shape;
+template <> struct Shape<false> {
+  static constexpr int kMax = kMaxBlock32;
+  static constexpr int kSlot = 1024;   // pack slot (>= kMax, multiple of 16)
+  // unpack per-block staging: a block starts up to 15 bytes into its first
+  // 16-byte chunk and its last chunk may run 15 bytes past its end
+  static constexpr int kStage = 1056;  // >= kMax + 30, multiple of 16
+};
+template <> struct Shape<true> {
+  static constexpr int kMax = kMaxBlock64;
+  static constexpr int kSlot = 2048;
+  static constexpr int kStage = 2080;
+};
+
+// ------------------------------------------------------------------------
+// small helpers
+// ------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v += shfl_xor64(v, d);
+  return v;
+}
+
+// Stream of block b: largest s with block_start[s] <= b (that stream is
+// non-empty).  Returns the first value index and the block's value count.
+__device__ __forceinline__ void block_span(const uint64_t* val_off, const uint64_t* bstart, int n_streams, int64_t b,
+                                           uint64_t* first, int* n) {
+  int lo = 0, hi = n_streams;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if ((int64_t)bstart[mid] <= b) lo = mid;
+    else hi = mid;
+  }
+  uint64_t f = val_off[lo] + (uint64_t)(b - (int64_t)bstart[lo]) * kBlock;
+  uint64_t e = val_off[lo + 1];
+  *first = f;
+  *n = (int)min((uint64_t)kBlock, e - f);
+}
+
+// Copy len bytes of a shared-memory slot (word aligned) to out[g..g+len):
+// whole 32-bit words where the global word lies inside the range, single
+// bytes at the two edges (those words are shared with neighbouring blocks).
+__device__ __forceinline__ void warp_copy_out(const uint32_t* sw, int len, uint8_t* out, uint64_t g, int lane) {
+  if (len <= 0) return;
+  const uint64_t ge = g + (uint64_t)len;
+  const uint64_t q0 = g >> 2, q1 = (ge + 3) >> 2;
+  for (uint64_t q = q0 + lane; q < q1; q += 32) {
+    const int64_t sb = (int64_t)(q * 4) - (int64_t)g;
+    if (sb >= 0 && sb + 4 <= len) {
+      const int qi = (int)(sb >> 2);
+      *(uint32_t*)(out + q * 4) = __funnelshift_r(sw[qi], sw[qi + 1], (int)(sb & 3) * 8);
+    } else {
+      for (int b = 0; b < 4; b++) {
+        const int64_t s = sb + b;
+        if (s >= 0 && s < len) out[q * 4 + b] = (uint8_t)(sw[s >> 2] >> ((s & 3) * 8));
+      }
+    }
+  }
+}
+
+// Stage global bytes [g0, g1) of buf (readable range [0, buf_len)) into
+// shared memory at dst16 (16-byte aligned) so that byte g0 lands at
+// dst16 + ((buf + g0) & 15).  Bytes outside the buffer read as zero.
+__device__ __forceinline__ void stage_bytes(uint4* dst16, const uint8_t* buf, uint64_t buf_len, uint64_t g0, uint64_t g1,
+                                            int tid, int nthr) {
+  const uintptr_t lo = (uintptr_t)buf, hi = lo + buf_len;
+  const uintptr_t a0 = (lo + g0) & ~(uintptr_t)15;
+  const uintptr_t a1 = (lo + g1 + 15) & ~(uintptr_t)15;
+  const int nch = (int)((a1 - a0) >> 4);
+  for (int c = tid; c < nch; c += nthr) {
+    const uintptr_t a = a0 + 16 * (uintptr_t)c;
+    uint4 v;
+    if (a >= lo && a + 16 <= hi) {
+      v = __ldcs((const uint4*)a);
+    } else {
+      uint32_t w[4] = {0, 0, 0, 0};
+      for (int b = 0; b < 16; b++) {
+        const uintptr_t x = a + b;
+        if (x >= lo && x < hi) w[b >> 2] |= (uint32_t)(*(const uint8_t*)x) << ((b & 3) * 8);
+      }
+      v = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    dst16[c] = v;
+  }
+}
+
+// ------------------------------------------------------------------------
+// planning
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) plan_kernel(const uint64_t* __restrict__ val_off, int n,
+                                                    uint64_t* __restrict__ bstart) {
+  __shared__ uint64_t warp_tot[32];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, T = blockDim.x;
+  const int64_t per = ((int64_t)n + T - 1) / T;
+  const int64_t s0 = min((int64_t)n, (int64_t)tid * per), s1 = min((int64_t)n, s0 + per);
+  uint64_t sum = 0;
+  for (int64_t s = s0; s < s1; s++) sum += (val_off[s + 1] - val_off[s] + kBlock - 1) / kBlock;
+  uint64_t incl = sum;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t lo = __shfl_up_sync(kFull, (uint32_t)incl, d), hi = __shfl_up_sync(kFull, (uint32_t)(incl >> 32), d);
+    if (lane >= d) incl += ((uint64_t)hi << 32) | lo;
+  }
+  if (lane == 31) warp_tot[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    uint64_t t = lane < (T >> 5) ? warp_tot[lane] : 0, ti = t;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t lo = __shfl_up_sync(kFull, (uint32_t)ti, d), hi = __shfl_up_sync(kFull, (uint32_t)(ti >> 32), d);
+      if (lane >= d) ti += ((uint64_t)hi << 32) | lo;
+    }
+    warp_tot[lane] = ti - t;
+  }
+  __syncthreads();
+  uint64_t acc = warp_tot[wid] + incl - sum;
+  for (int64_t s = s0; s < s1; s++) {
+    bstart[s] = acc;
+    acc += (val_off[s + 1] - val_off[s] + kBlock - 1) / kBlock;
+  }
+  if (tid == T - 1) bstart[n] = acc;
+}
+
+__global__ void stream_off_kernel(const uint64_t* __restrict__ block_off, const uint64_t* __restrict__ bstart, int n,
+                                  uint64_t* __restrict__ sbo) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s <= n) sbo[s] = block_off[bstart[s]];
+}
+
+// ------------------------------------------------------------------------
+// batched pack with single-pass decoupled look-back
+// ------------------------------------------------------------------------
+// Tile state word: bits 0-1 flag (0 empty, 1 aggregate, 2 inclusive
+// prefix), bits 2-63 value.  Waits are bounded; on expiry the kernel
+// records UTL_ERR_TIMEOUT and carries on with a zero contribution so it
+// always terminates.  Tiles are handed out in launch order by an atomic
+// counter, so every predecessor of a waiting tile is already running.
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+__device__ uint64_t tile_lookback(uint64_t* status, int64_t tile, uint64_t agg, int lane, uint32_t* err) {
+  if (tile == 0) {
+    if (lane == 0) st_relaxed_u64(&status[0], (agg << 2) | 2u);
+    return 0;
+  }
+  if (lane == 0) st_relaxed_u64(&status[tile], (agg << 2) | 1u);
+  uint64_t excl = 0;
+  int64_t j = tile - 1;
+  bool timed_out = false;
+  for (;;) {
+    const int64_t idx = j - lane;
+    uint64_t s = 2u;  // before tile 0: an inclusive prefix of zero
+    if (idx >= 0) {
+      uint32_t it = 0;
+      s = ld_relaxed_u64(&status[idx]);
+      while ((s & 3u) == 0) {
+        if (++it > kSpinLimit) {
+          timed_out = true;
+          s = 2u;
+          break;
+        }
+        __nanosleep(64);
+        s = ld_relaxed_u64(&status[idx]);
+      }
+    }
+    const unsigned pm = __ballot_sync(kFull, (s & 3u) == 2u);
+    const int first = pm ? __ffs(pm) - 1 : 32;
+    excl += warp_sum_u64(lane <= first ? (s >> 2) : 0ull);
+    if (pm) break;
+    j -= 32;
+  }
+  if (__any_sync(kFull, timed_out) && lane == 0 && err) atomicOr(err, 1u << 10);
+  if (lane == 0) st_relaxed_u64(&status[tile], ((excl + agg) << 2) | 2u);
+  return excl;
+}
+
+template <bool U64>
+__global__ void __launch_bounds__(kThreads) pack_kernel(PackArgs a) {
+  extern __shared__ uint4 smem4[];
+  constexpr int kSlot = Shape<U64>::kSlot;
+  uint8_t* slots = (uint8_t*)smem4;
+  uint32_t* hb_all = (uint32_t*)(slots + kTile * kSlot + 16);
+  __shared__ int s_len[kTile];
+  __shared__ int s_off[kTile];
+  __shared__ int64_t s_tile;
+  __shared__ uint64_t s_prefix;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t* hb = hb_all + warp * kBlock;
+
+  for (;;) {
+    if (tid == 0) s_tile = (int64_t)atomicAdd((unsigned long long*)a.counter, 1ull);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    if (tile >= a.n_tiles) break;
+    const int64_t b0 = tile * kTile;
+
+#pragma unroll
+    for (int j = 0; j < kBlocksPerWarp; j++) {
+      const int lb = warp * kBlocksPerWarp + j;
+      const int64_t b = b0 + lb;
+      int len = 0;
+      if (b < a.n_blocks) {
+        uint64_t first;
+        int n;
+        block_span(a.val_off, a.block_start, a.n_streams, b, &first, &n);
+        if (U64) {
+          const uint64_t* vp = (const uint64_t*)a.values + first;
+          uint64_t x[4];
+#pragma unroll
+          for (int k = 0; k < 4; k++) x[k] = (lane + 32 * k < n) ? __ldcs(vp + lane + 32 * k) : 0ull;
+          len = warp_pack_block64(x, n, a.flag, slots, lb * kSlot, hb, lane);
+        } else {
+          const uint32_t* vp = (const uint32_t*)a.values + first;
+          uint32_t v[4];
+#pragma unroll
+          for (int k = 0; k < 4; k++) v[k] = (lane + 32 * k < n) ? __ldcs(vp + lane + 32 * k) : 0u;
+          len = warp_pack_block(v, n, a.flag, kTypeU32, kModePlain, 0, slots, lb * kSlot, hb, lane);
+        }
+      }
+      if (lane == 0) s_len[lb] = len;
+    }
+    __syncthreads();
+
+    if (warp == 0) {
+      const int l = lane < kTile ? s_len[lane] : 0;
+      const int incl = warp_incl_scan(l, lane);
+      if (lane < kTile) s_off[lane] = incl - l;
+      const uint64_t agg = (uint64_t)__shfl_sync(kFull, incl, 31);
+      const uint64_t prefix = tile_lookback(a.tile_status, tile, agg, lane, a.err);
+      if (lane == 0) s_prefix = prefix;
+    }
+    __syncthreads();
+
+    const uint64_t prefix = s_prefix;
+#pragma unroll
+    for (int j = 0; j < kBlocksPerWarp; j++) {
+      const int lb = warp * kBlocksPerWarp + j;
+      const int64_t b = b0 + lb;
+      if (b < a.n_blocks) {
+        const uint64_t g = prefix + (uint64_t)s_off[lb];
+        const int len = s_len[lb];
+        if (g + (uint64_t)len <= a.out_cap) {
+          warp_copy_out((const uint32_t*)(slots + lb * kSlot), len, a.out, g, lane);
+        } else if (lane == 0 && a.err) {
+          atomicOr(a.err, 1u << 9);
+        }
+        if (lane == 0) {
+          a.block_off[b] = g;
+          if (b == a.n_blocks - 1) a.block_off[a.n_blocks] = g + (uint64_t)len;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------------
+// batched unpack
+// ------------------------------------------------------------------------
+template <bool U64>
+__global__ void __launch_bounds__(kThreads) unpack_kernel(UnpackArgs a) {
+  extern __shared__ uint4 smem4[];
+  constexpr int kStage = Shape<U64>::kStage;
+  constexpr int kMax = Shape<U64>::kMax;
+  uint8_t* stage = (uint8_t*)smem4;
+  uint32_t* hb_all = (uint32_t*)(stage + kTile * kStage + 64);
+  __shared__ uint64_t s_boff[kTile + 1];
+  __shared__ int s_contig;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t* hb = hb_all + warp * kBlock;
+  const int64_t b0 = (int64_t)blockIdx.x * kTile;
+  const int nb = (int)min((int64_t)kTile, a.n_blocks - b0);
+
+  if (tid <= nb) s_boff[tid] = a.block_off[b0 + tid];
+  __syncthreads();
+  if (tid == 0) {
+    int ok = 1;
+    for (int j = 0; j < nb; j++) {
+      const uint64_t s = s_boff[j], e = s_boff[j + 1];
+      if (e < s || e - s > (uint64_t)kMax || e > a.packed_len) ok = 0;
+    }
+    s_contig = ok;
+  }
+  __syncthreads();
+  const bool contig = s_contig != 0;
+  if (contig) {
+    stage_bytes(smem4, a.packed, a.packed_len, s_boff[0], s_boff[nb], tid, kThreads);
+  } else {
+    for (int j = warp; j < nb; j += kWarps) {
+      const uint64_t s = s_boff[j], e = s_boff[j + 1];
+      if (e >= s && e - s <= (uint64_t)kMax && e <= a.packed_len)
+        stage_bytes((uint4*)(stage + j * kStage), a.packed, a.packed_len, s, e, lane, 32);
+    }
+  }
+  __syncthreads();
+
+  const SmemBytes sb{(const uint32_t*)stage};
+  const int base0 = (int)(((uintptr_t)a.packed + s_boff[0]) & 15);
+#pragma unroll
+  for (int j = 0; j < kBlocksPerWarp; j++) {
+    const int lb = warp * kBlocksPerWarp + j;
+    if (lb >= nb) break;
+    const int64_t b = b0 + lb;
+    const uint64_t s = s_boff[lb], e = s_boff[lb + 1];
+    uint64_t first;
+    int want;
+    block_span(a.val_off, a.block_start, a.n_streams, b, &first, &want);
+    int status = kOK, ovf = 0;
+    if (e < s || e - s > (uint64_t)kMax || e > a.packed_len) {
+      status = kErrCountMismatch;
+    } else {
+      const int len = (int)(e - s);
+      const int blk = contig ? base0 + (int)(s - s_boff[0])
+                             : lb * kStage + (int)(((uintptr_t)a.packed + s) & 15);
+      UnpackResult r;
+      if (U64) {
+        uint64_t x[4];
+        r = warp_unpack_block64(sb, blk, len, x, hb, lane);
+        if (r.status == kOK && (r.count != want || r.consumed != len)) r.status = kErrCountMismatch;
+        if (r.status == kOK) {
+          uint64_t* op = (uint64_t*)a.values + first;
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+            if (lane + 32 * k < want) __stcs(op + lane + 32 * k, x[k]);
+        }
+      } else {
+        uint32_t v[4];
+        r = warp_unpack_block(sb, blk, len, false, v, hb, lane);
+        if (r.status == kOK && (r.count != want || r.consumed != len)) r.status = kErrCountMismatch;
+        if (r.status == kOK) {
+          uint32_t* op = (uint32_t*)a.values + first;
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+            if (lane + 32 * k < want) __stcs(op + lane + 32 * k, v[k]);
+        }
+      }
+      status = r.status;
+      ovf = r.ovf;
+    }
+    if (lane == 0) {
+      if (a.block_status) a.block_status[b] = status | (ovf << 8);
+      if (status != kOK && a.err) atomicOr(a.err, 1u << status);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Get: one thread per query; queries that need the reference's full-block
+// fallback (delta blocks, deep positions) are resolved by the whole warp.
+// ------------------------------------------------------------------------
+struct SubGet {
+  const uint8_t* p;  // sub-block start
+  int64_t rd;        // readable bytes
+  int64_t len;       // the reference's len(src)
+  int pos;
+};
+
+// Resolve every lane whose r.need_full is set with a warp-wide unpack of
+// its block (getUint32FullUnpack / getFullUnpackViaBlock, get.go:198-218,
+// 339-349), bounded by the block end the thread validated.
+template <bool U64>
+__device__ __forceinline__ void resolve_full(bool active, const SubGet& q, GetResult& r, uint32_t* hb, int lane) {
+  unsigned m = __ballot_sync(kFull, active && r.need_full);
+  while (m) {
+    const int src = __ffs(m) - 1;
+    m &= m - 1;
+    const uint8_t* p = (const uint8_t*)__shfl_sync(kFull, (unsigned long long)q.p, src);
+    const int64_t rd = (int64_t)__shfl_sync(kFull, (unsigned long long)q.rd, src);
+    const int64_t len = (int64_t)__shfl_sync(kFull, (unsigned long long)r.end, src);
+    const int pos = __shfl_sync(kFull, q.pos, src);
+    uint32_t v[4];
+    const GlobalBytes g{p, rd};
+    const UnpackResult u = warp_unpack_block(g, 0, len, U64, v, hb, lane);
+    const int slot = pos >> 5;
+    uint32_t mine = slot == 0 ? v[0] : slot == 1 ? v[1] : slot == 2 ? v[2] : v[3];
+    const uint32_t val = __shfl_sync(kFull, mine, pos & 31);
+    if (lane == src) {
+      r.need_full = false;
+      r.status = u.status;
+      r.ovf = u.ovf;
+      r.value = val;
+    }
+  }
+}
+
+template <bool U64>
+__global__ void __launch_bounds__(kThreads) get_kernel(GetArgs a) {
+  __shared__ uint32_t hb_all[kWarps * kBlock];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t* hb = hb_all + warp * kBlock;
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = q < a.n_queries;
+
+  int status = kOK, ovf = 0;
+  uint64_t result = 0;
+  SubGet sg{nullptr, 0, 0, 0};
+  bool live = false;
+  if (act) {
+    const uint32_t s = a.q_stream[q];
+    const uint64_t p = a.q_pos[q];
+    if (s >= (uint32_t)a.n_streams || p >= a.val_off[s + 1] - a.val_off[s]) {
+      status = kErrPositionOutOfRange;
+    } else {
+      const int64_t b = (int64_t)a.block_start[s] + (int64_t)(p / kBlock);
+      const uint64_t off = a.block_off[b], end = a.block_off[b + 1];
+      const uint64_t e2 = min(end, a.packed_len);
+      const int64_t rd = (e2 > off) ? (int64_t)(e2 - off) : 0;
+      sg = SubGet{a.packed + off, rd, (end >= off) ? (int64_t)(end - off) : 0, (int)(p % kBlock)};
+      live = true;
+    }
+  }
+
+  if (!U64) {
+    GetResult r{kOK, 0, 0u, false};
+    if (live) r = thread_get_u32(GlobalBytes{sg.p, sg.rd}, sg.len, sg.pos, false);
+    resolve_full<false>(live, sg, r, hb, lane);
+    if (live) {
+      status = r.status;
+      ovf = r.ovf;
+      result = r.value;
+    }
+  } else {
+    // getUint64Scalar, uint64.go:372-436
+    const GlobalBytes g{sg.p, sg.rd};
+    uint32_t h = 0;
+    bool go = live;
+    if (go) {
+      if (sg.len < 4) { status = kErrInvalidBuffer; go = false; }
+      else {
+        h = g.u32(0);
+        if (((h >> 13) & 3) != 3) { status = kErrUnsupportedType; go = false; }
+      }
+    }
+    GetResult r{kOK, 0, 0u, false};
+    if (go) r = thread_get_u32(g, sg.len, sg.pos, true);
+    resolve_full<true>(go, sg, r, hb, lane);
+    if (go && r.status != kOK) { status = r.status; ovf = r.ovf; go = false; }
+    const uint32_t lower = r.value;
+    const int forw = (int)((h >> 15) & 3), exc = (int)(h >> 24);
+    SubGet sg2{nullptr, 0, 0, sg.pos};
+    bool second = false;
+    if (go) {
+      if (!(h & kHdrCombine)) {
+        uint64_t base = 0;
+        if (forw == 3) {
+          const int off = 4 + (exc > 0 ? 2 : 0);
+          if (sg.len < off + 8) { status = kErrInvalidBuffer; go = false; }
+          else base = g.u64(off);
+        }
+        if (go) result = (uint64_t)lower + base;
+      } else {
+        const int64_t meta = 4 + (exc > 0 ? 2 : 0) + ((1 << forw) >> 1) + 2;
+        if (sg.len < meta) { status = kErrInvalidBuffer; go = false; }
+        else {
+          const int64_t b2len = g.u16(meta - 2);
+          int64_t b1 = meta + (int64_t)(((h >> 8) & 31) * 4) * 16;
+          if (exc > 0) b1 += min(exc, 16) + (int64_t)g.u16(4);
+          if (b1 + b2len > sg.len) { status = kErrInvalidBuffer; go = false; }
+          else {
+            const int64_t rd2 = max((int64_t)0, min(b2len, sg.rd - b1));
+            sg2 = SubGet{sg.p + b1, rd2, b2len, sg.pos};
+            second = true;
+          }
+        }
+      }
+    }
+    GetResult r2{kOK, 0, 0u, false};
+    if (second) r2 = thread_get_u32(GlobalBytes{sg2.p, sg2.rd}, sg2.len, sg2.pos, true);
+    resolve_full<true>(second, sg2, r2, hb, lane);
+    if (second) {
+      if (r2.status != kOK) { status = r2.status; ovf = r2.ovf; }
+      else result = ((uint64_t)r2.value << 32) | lower;
+    }
+  }
+
+  if (act) {
+    if (U64) ((uint64_t*)a.out)[q] = status == kOK ? result : 0ull;
+    else ((uint32_t*)a.out)[q] = status == kOK ? (uint32_t)result : 0u;
+    if (a.status) a.status[q] = status | (ovf << 8);
+    if (status != kOK && a.err) atomicOr(a.err, 1u << status);
+  }
+}
+
+// ------------------------------------------------------------------------
+// per-call kernels (one warp): inputs and outputs live in mapped pinned
+// host memory, so a call is one launch and one synchronize.
+// ------------------------------------------------------------------------
+template <bool U64>
+__global__ void __launch_bounds__(32) plain_pack_kernel(int flag, const void* vals, int n, uint8_t* out,
+                                                        PlainResult* res) {
+  __shared__ uint4 slot4[(Shape<U64>::kSlot + 16) / 16];
+  __shared__ uint32_t hb[kBlock];
+  const int lane = threadIdx.x;
+  uint8_t* slot = (uint8_t*)slot4;
+  int len;
+  if (U64) {
+    const uint64_t* vp = (const uint64_t*)vals;
+    uint64_t x[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) x[k] = (lane + 32 * k < n) ? vp[lane + 32 * k] : 0ull;
+    len = warp_pack_block64(x, n, flag, slot, 0, hb, lane);
+  } else {
+    const uint32_t* vp = (const uint32_t*)vals;
+    uint32_t v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) v[k] = (lane + 32 * k < n) ? vp[lane + 32 * k] : 0u;
+    len = warp_pack_block(v, n, flag, kTypeU32, kModePlain, 0, slot, 0, hb, lane);
+  }
+  __syncwarp();
+  warp_copy_out((const uint32_t*)slot, len, out, 0, lane);
+  if (lane == 0) {
+    res->status = kOK;
+    res->len = len;
+  }
+}
+
+// Copy staged bytes from mapped host memory into device scratch, then
+// decode from device memory.
+__device__ __forceinline__ void warp_stage_dev(const uint8_t* src, int64_t n, uint8_t* tmp, int lane) {
+  for (int64_t i = lane; i < n; i += 32) tmp[i] = src[i];
+  __syncwarp();
+  __threadfence_block();
+}
+
+template <bool U64>
+__global__ void __launch_bounds__(32) plain_unpack_kernel(const uint8_t* src, int64_t staged, int64_t avail,
+                                                          uint8_t* tmp, void* vals, PlainResult* res) {
+  __shared__ uint32_t hb[kBlock];
+  const int lane = threadIdx.x;
+  warp_stage_dev(src, staged, tmp, lane);
+  const GlobalBytes g{tmp, staged};
+  UnpackResult r;
+  if (U64) {
+    uint64_t x[4];
+    r = warp_unpack_block64(g, 0, avail, x, hb, lane);
+    if (r.status == kOK) {
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        if (lane + 32 * k < r.count) ((uint64_t*)vals)[lane + 32 * k] = x[k];
+    }
+  } else {
+    uint32_t v[4];
+    r = warp_unpack_block(g, 0, avail, false, v, hb, lane);
+    if (r.status == kOK) {
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        if (lane + 32 * k < r.count) ((uint32_t*)vals)[lane + 32 * k] = v[k];
+    }
+  }
+  if (lane == 0) {
+    res->status = r.status;
+    res->count = r.count;
+    res->len = r.consumed;
+    res->ovf = r.ovf;
+  }
+}
+
+template <bool U64>
+__global__ void __launch_bounds__(32) plain_get_kernel(int pos, const uint8_t* src, int64_t staged, int64_t avail,
+                                                       uint8_t* tmp, PlainResult* res) {
+  __shared__ uint32_t hb[kBlock];
+  const int lane = threadIdx.x;
+  warp_stage_dev(src, staged, tmp, lane);
+  const GlobalBytes g{tmp, staged};
+  const bool me = lane == 0;
+  int status = kOK, ovf = 0;
+  uint64_t result = 0;
+  if (!U64) {
+    SubGet sg{tmp, staged, avail, pos};
+    GetResult r{kOK, 0, 0u, false};
+    if (me) r = thread_get_u32(g, avail, pos, false);
+    resolve_full<false>(me, sg, r, hb, lane);
+    status = r.status;
+    ovf = r.ovf;
+    result = r.value;
+  } else {
+    uint32_t h = 0;
+    bool go = true;
+    if (avail < 4) { status = kErrInvalidBuffer; go = false; }
+    else {
+      h = g.u32(0);
+      if (((h >> 13) & 3) != 3) { status = kErrUnsupportedType; go = false; }
+    }
+    SubGet sg{tmp, staged, avail, pos};
+    GetResult r{kOK, 0, 0u, false};
+    if (go && me) r = thread_get_u32(g, avail, pos, true);
+    resolve_full<true>(go && me, sg, r, hb, lane);
+    if (go && r.status != kOK) { status = r.status; ovf = r.ovf; go = false; }
+    const int forw = (int)((h >> 15) & 3), exc = (int)(h >> 24);
+    bool second = false;
+    SubGet sg2{nullptr, 0, 0, pos};
+    if (go) {
+      if (!(h & kHdrCombine)) {
+        uint64_t base = 0;
+        if (forw == 3) {
+          const int off = 4 + (exc > 0 ? 2 : 0);
+          if (avail < off + 8) { status = kErrInvalidBuffer; go = false; }
+          else base = g.u64(off);
+        }
+        if (go) result = (uint64_t)r.value + base;
+      } else {
+        const int64_t meta = 4 + (exc > 0 ? 2 : 0) + ((1 << forw) >> 1) + 2;
+        if (avail < meta) { status = kErrInvalidBuffer; go = false; }
+        else {
+          const int64_t b2len = g.u16(meta - 2);
+          int64_t b1 = meta + (int64_t)(((h >> 8) & 31) * 4) * 16;
+          if (exc > 0) b1 += min(exc, 16) + (int64_t)g.u16(4);
+          if (b1 + b2len > avail) { status = kErrInvalidBuffer; go = false; }
+          else {
+            sg2 = SubGet{tmp + b1, max((int64_t)0, min(b2len, staged - b1)), b2len, pos};
+            second = true;
+          }
+        }
+      }
+    }
+    GetResult r2{kOK, 0, 0u, false};
+    if (second && me) r2 = thread_get_u32(GlobalBytes{sg2.p, sg2.rd}, sg2.len, pos, true);
+    resolve_full<true>(second && me, sg2, r2, hb, lane);
+    if (second) {
+      if (r2.status != kOK) { status = r2.status; ovf = r2.ovf; }
+      else result = ((uint64_t)r2.value << 32) | r.value;
+    }
+  }
+  if (me) {
+    res->status = status;
+    res->ovf = ovf;
+    res->value = status == kOK ? result : 0ull;
+  }
+}
+
+// ------------------------------------------------------------------------
+// host launchers
+// ------------------------------------------------------------------------
+namespace launch {
+
+static int g_num_sms = 0;
+static int g_pack_ctas_per_sm[2] = {0, 0};
+
+static int num_sms() {
+  if (g_num_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+size_t pack_smem(bool u64) {
+  return (size_t)kTile * (u64 ? Shape<true>::kSlot : Shape<false>::kSlot) + 16 + (size_t)kWarps * kBlock * 4;
+}
+size_t unpack_smem(bool u64) {
+  return (size_t)kTile * (u64 ? Shape<true>::kStage : Shape<false>::kStage) + 64 + (size_t)kWarps * kBlock * 4;
+}
+
+int64_t tiles_for(int64_t n_blocks) { return (n_blocks + kTile - 1) / kTile; }
+
+cudaError_t plan(const uint64_t* val_off, int n, uint64_t* bstart, cudaStream_t st) {
+  plan_kernel<<<1, 1024, 0, st>>>(val_off, n, bstart);
+  note_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t stream_offsets(const uint64_t* block_off, const uint64_t* bstart, int n, uint64_t* sbo, cudaStream_t st) {
+  int threads = 256, blocks = (n + 1 + threads - 1) / threads;
+  stream_off_kernel<<<blocks, threads, 0, st>>>(block_off, bstart, n, sbo);
+  note_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t pack(bool u64, const PackArgs& a, cudaStream_t st) {
+  const size_t smem = pack_smem(u64);
+  const int idx = u64 ? 1 : 0;
+  if (g_pack_ctas_per_sm[idx] == 0) {
+    cudaError_t e;
+    if (u64) {
+      e = cudaFuncSetAttribute(pack_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_pack_ctas_per_sm[idx], pack_kernel<true>, kThreads, smem);
+    } else {
+      e = cudaFuncSetAttribute(pack_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_pack_ctas_per_sm[idx], pack_kernel<false>, kThreads, smem);
+    }
+    if (g_pack_ctas_per_sm[idx] <= 0) g_pack_ctas_per_sm[idx] = 1;
+  }
+  int64_t grid = (int64_t)num_sms() * g_pack_ctas_per_sm[idx];
+  if (grid > a.n_tiles) grid = a.n_tiles;
+  if (grid < 1) grid = 1;
+  if (u64) pack_kernel<true><<<(unsigned)grid, kThreads, smem, st>>>(a);
+  else pack_kernel<false><<<(unsigned)grid, kThreads, smem, st>>>(a);
+  note_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
+  const size_t smem = unpack_smem(u64);
+  static bool configured[2] = {false, false};
+  const int idx = u64 ? 1 : 0;
+  if (!configured[idx]) {
+    cudaError_t e = u64 ? cudaFuncSetAttribute(unpack_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                        : cudaFuncSetAttribute(unpack_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured[idx] = true;
+  }
+  const int64_t grid = tiles_for(a.n_blocks);
+  if (grid <= 0) return cudaSuccess;
+  if (u64) unpack_kernel<true><<<(unsigned)grid, kThreads, smem, st>>>(a);
+  else unpack_kernel<false><<<(unsigned)grid, kThreads, smem, st>>>(a);
+  note_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t get(bool u64, const GetArgs& a, cudaStream_t st) {
+  if (a.n_queries <= 0) return cudaSuccess;
+  const int64_t grid = (a.n_queries + kThreads - 1) / kThreads;
+  if (u64) get_kernel<true><<<(unsigned)grid, kThreads, 0, st>>>(a);
+  else get_kernel<false><<<(unsigned)grid, kThreads, 0, st>>>(a);
+  note_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t plain_pack(bool u64, int flag, const void* vals, int n, uint8_t* out, PlainResult* res, cudaStream_t st) {
+  if (u64) plain_pack_kernel<true><<<1, 32, 0, st>>>(flag, vals, n, out, res);
+  else plain_pack_kernel<false><<<1, 32, 0, st>>>(flag, vals, n, out, res);
+  note_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t plain_unpack(bool u64, const uint8_t* src, int64_t staged, int64_t avail, uint8_t* tmp, void* vals,
+                         PlainResult* res, cudaStream_t st) {
+  if (u64) plain_unpack_kernel<true><<<1, 32, 0, st>>>(src, staged, avail, tmp, vals, res);
+  else plain_unpack_kernel<false><<<1, 32, 0, st>>>(src, staged, avail, tmp, vals, res);
+  note_launch(1);
+  return cudaGetLastError();
+}
+
+cudaError_t plain_get(bool u64, int pos, const uint8_t* src, int64_t staged, int64_t avail, uint8_t* tmp,
+                      PlainResult* res, cudaStream_t st) {
+  if (u64) plain_get_kernel<true><<<1, 32, 0, st>>>(pos, src, staged, avail, tmp, res);
+  else plain_get_kernel<false><<<1, 32, 0, st>>>(pos, src, staged, avail, tmp, res);
+  note_launch(1);
+  return cudaGetLastError();
+}
+
+}  // namespace launch
+}  // namespace utl
