@@ -1,0 +1,475 @@
+#!/usr/bin/env python
+"""Benchmark of the batched UTL-PFOR codec on B200.
+
+One step = one batched PackUint32 pass over the whole workload followed by
+one batched UnpackUint32 pass over the packed result (a round trip),
+inputs resident in HBM.  The default workload is the exception-heavy
+configuration: 2^28 uint32 values in 2^21 blocks of 128, values uniform in
+[0, 2^8) except with probability 0.02 uniform in [2^8, 2^32), and 10% of
+blocks all-equal (constant drawn uniform in [0, 2^8)), flag 0, seeded
+synthetic data.  The working set (1 GiB of values in, 1 GiB out) is far
+larger than L2, so no L2 flush is needed between steps.
+
+Printed: ONE JSON line (rank 0).  value = uncompressed round-trip
+throughput (bytes of values packed + bytes of values unpacked) / step
+time, summed over ranks.  e2e = the same metric through the host-buffer
+C-ABI calls (utl_pack_streams_u32 / utl_unpack_streams_u32) with pinned
+host memory, copies included.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload c3|c3-nofor|c3-nopatch|c1|c2|c4]
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DELTA, NOFOR, NOPATCH = 1, 2, 4
+L2_BYTES = 126 * 2**20
+
+
+# --------------------------------------------------------------------------
+# workloads (seeded synthetic data with the configs' shapes)
+# --------------------------------------------------------------------------
+WORKLOADS = {
+    "c3": dict(desc="pfor_exception_heavy: 2^28 u32 in 2^21 blocks, U[0,2^8) + 2% U[2^8,2^32), "
+                    "10% all-equal blocks", flag=0, is64=False),
+    "c3-nofor": dict(desc="pfor_exception_heavy (flag NoFOR)", flag=NOFOR, is64=False),
+    "c3-nopatch": dict(desc="pfor_exception_heavy (flag NoPatch)", flag=NOPATCH, is64=False),
+    "c1": dict(desc="plain_round_trip: 2^20 u32 uniform [0,2^11), flag 0", flag=0, is64=False),
+    "c2": dict(desc="delta_posting_lists: 1000 lists log-uniform [128,2^20], gaps 1+Geom(1/64), flag Delta",
+               flag=DELTA, is64=False),
+    "c4": dict(desc="uint64_streams: 2^26 u64 in 512 streams, 1/3 FOR-reducible, 1/3 full-range, "
+                    "1/3 random walks from 2^62 (flag Delta)", flag=DELTA, is64=True),
+}
+
+
+def gen_c3_torch(torch, n, gen, dev):
+    v = torch.randint(0, 256, (n,), device=dev, dtype=torch.int32, generator=gen)
+    m = torch.rand(n, device=dev, generator=gen) < 0.02
+    big = torch.randint(256, 2**32, (n,), device=dev, dtype=torch.int64, generator=gen).to(torch.int32)
+    v = torch.where(m, big, v)
+    del big, m
+    nb = n // 128
+    sel = torch.rand(nb, device=dev, generator=gen) < 0.10
+    c = torch.randint(0, 256, (nb,), device=dev, dtype=torch.int32, generator=gen)
+    vb = v.view(nb, 128)
+    vb.copy_(torch.where(sel[:, None], c[:, None], vb))
+    return v
+
+
+def loguniform_lengths(rng, n, lo, hi):
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), n)).astype(np.int64)
+
+
+def make_workload(torch, name, rank, dev, log2n=28):
+    """Returns (values CUDA tensor, val_off numpy uint64)."""
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    rng = np.random.default_rng(1234 + rank)
+    if name.startswith("c3"):
+        n = 1 << log2n
+        return gen_c3_torch(torch, n, gen, dev), np.array([0, n], dtype=np.uint64)
+    if name == "c1":
+        n = 1 << 20
+        v = torch.randint(0, 2**11, (n,), device=dev, dtype=torch.int32, generator=gen)
+        return v, np.array([0, n], dtype=np.uint64)
+    if name == "c2":
+        lens = loguniform_lengths(rng, 1000, 128, 2**20)
+        vo = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+        n = int(vo[-1])
+        gaps = 1 + torch.distributions.Geometric(probs=torch.tensor(1 / 64, device=dev)).sample((n,)).to(torch.int64)
+        # per-list cumulative sums: global cumsum minus the list's starting prefix
+        cs = torch.cumsum(gaps, 0)
+        starts = torch.from_numpy(vo[:-1].astype(np.int64)).to(dev)
+        base = torch.where(starts > 0, cs[(starts - 1).clamp(min=0)], torch.zeros_like(starts))
+        rep = torch.repeat_interleave(base, torch.from_numpy(lens).to(dev))
+        v = (cs - rep).to(torch.int32)
+        return v, vo
+    if name == "c4":
+        lens = loguniform_lengths(rng, 512, 128, 2**18).astype(np.float64)
+        lens = np.maximum(128, np.round(lens * (2**26 / lens.sum()))).astype(np.int64)
+        vo = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+        parts = []
+        for s, ln in enumerate(lens):
+            ln = int(ln)
+            kind = s % 3
+            if kind == 0:
+                x = (2**40 + torch.randint(0, 2**20, (ln,), device=dev, dtype=torch.int64, generator=gen))
+            elif kind == 1:
+                x = torch.randint(-2**63, 2**63 - 1, (ln,), device=dev, dtype=torch.int64, generator=gen)
+            else:
+                steps = torch.randint(-1000, 1001, (ln,), device=dev, dtype=torch.int64, generator=gen)
+                x = 2**62 + torch.cumsum(steps, 0)
+            parts.append(x)
+        return torch.cat(parts), vo
+    raise ValueError(name)
+
+
+# --------------------------------------------------------------------------
+# clocks sampled during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu_id), "--query-gpu=" + self.QUERY, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def gpu_smi_id(torch, dev_index):
+    try:
+        bus = torch.cuda.get_device_properties(dev_index).pci_bus_id
+        if bus:
+            return bus
+    except Exception:
+        pass
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        return vis.split(",")[dev_index]
+    return dev_index
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per value of the pack and unpack kernels from the
+    committed ncu summary (profiles/*.txt lines 'traffic_per_value <kernel> <bytes>')."""
+    out = {}
+    d = os.path.join(ROOT, "profiles")
+    if os.path.isdir(d):
+        for fn in sorted(os.listdir(d)):
+            if not fn.endswith(".txt"):
+                continue
+            with open(os.path.join(d, fn)) as f:
+                for ln in f:
+                    p = ln.split()
+                    if len(p) == 3 and p[0] == "traffic_per_value":
+                        try:
+                            out[p[1]] = float(p[2])
+                        except ValueError:
+                            pass
+    return out
+
+
+# --------------------------------------------------------------------------
+# CPU side: the oracle restatement timed on the host cores
+# --------------------------------------------------------------------------
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_round_trip(values_np, val_off, flag, threads, min_seconds=10.0, max_rounds=50, rounds=None):
+    """Pack + unpack the sample with the oracle on `threads` host threads.
+    Returns (list of per-round seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_ref as O
+    times = []
+    t_start = time.perf_counter()
+    while True:
+        t0 = time.perf_counter()
+        packed, bo, _ = O.pack_streams(flag, values_np, val_off, n_threads=threads)
+        out, err = O.unpack_streams(packed, bo, val_off, dtype=values_np.dtype, n_threads=threads)
+        t1 = time.perf_counter()
+        assert err == 0
+        times.append(t1 - t0)
+        if rounds is not None:
+            if len(times) >= rounds:
+                break
+        elif time.perf_counter() - t_start >= min_seconds or len(times) >= max_rounds:
+            break
+    return times
+
+
+def c3_sample_host(n, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.integers(0, 256, n, dtype=np.uint64)
+    m = rng.random(n) < 0.02
+    v[m] = rng.integers(256, 2**32, int(m.sum()), dtype=np.uint64)
+    v = v.astype(np.uint32)
+    nb = n // 128
+    sel = rng.random(nb) < 0.10
+    c = rng.integers(0, 256, nb, dtype=np.uint64).astype(np.uint32)
+    vb = v.reshape(nb, 128)
+    vb[sel] = c[sel][:, None]
+    return v
+
+
+# --------------------------------------------------------------------------
+def run_reference(args):
+    """The reference arm: the reference's CPU algorithm (the oracle's plain-C
+    restatement; the Go reference has no toolchain here) on the host cores,
+    same metric and workload shape, each step one bounded sample."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wl = WORKLOADS[args.workload]
+    threads = host_threads()
+    S = 1 << 24
+    vals = c3_sample_host(S, 99)
+    vo = np.array([0, S], dtype=np.uint64)
+    cpu_round_trip(vals, vo, wl["flag"], threads, rounds=max(args.warmup, 1))
+    times = cpu_round_trip(vals, vo, wl["flag"], threads, rounds=args.steps)
+    t = sum(times) / len(times)
+    gbps = 2 * 4 * S / t / 1e9
+    sample = "%d u32 values (%d MiB) of the workload's distribution per step" % (S, 4 * S >> 20)
+    line = {"metric": "round-trip uncompressed GB/s (batched PackUint32 + UnpackUint32)", "value": gbps,
+            "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic (seeded, workload distribution)",
+            "config": {"workload": wl["desc"], "flag": wl["flag"], "sample_values": S},
+            "cpu_baseline": {"value": gbps, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": gbps, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--log2n", type=int, default=28, help="values per GPU of the c3 workloads (2^log2n)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import utlpfor_b200 as U
+    from utlpfor_b200._lib import load
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    wl = WORKLOADS[args.workload]
+    flag, is64 = wl["flag"], wl["is64"]
+    esz = 8 if is64 else 4
+    values, vo = make_workload(torch, args.workload, rank, dev, args.log2n)
+    n = int(vo[-1])
+    codec = U.BatchCodec(vo, flag=flag, is64=is64, device=dev)
+    out = torch.empty_like(values)
+    L = load()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # correctness of the timed path: one checked round trip
+    codec.pack(values)
+    codec.unpack(out)
+    torch.cuda.synchronize()
+    assert codec.error_bits() == 0, "device reported errors"
+    assert torch.equal(out, values), "round trip mismatch"
+    packed_len = codec.packed_len
+
+    for _ in range(args.warmup):
+        codec.pack(values)
+        codec.unpack(out)
+    barrier()
+    sampler = ClockSampler(gpu_smi_id(torch, local))
+    sampler.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = L.utl_launch_count()
+    barrier()
+    t_all0 = torch.cuda.Event(enable_timing=True)
+    t_all1 = torch.cuda.Event(enable_timing=True)
+    t_all0.record()
+    for e0, e1, e2 in ev:
+        e0.record()
+        codec.pack(values)
+        e1.record()
+        codec.unpack(out)
+        e2.record()
+    t_all1.record()
+    barrier()
+    launches = L.utl_launch_count() - launches0
+    clocks = sampler.stop()
+    total_ms = t_all0.elapsed_time(t_all1)
+    pack_ms = sum(a.elapsed_time(b) for a, b, _ in ev) / args.steps
+    unpack_ms = sum(b.elapsed_time(c) for _, b, c in ev) / args.steps
+    step_ms = total_ms / args.steps
+    if world > 1:
+        t = torch.tensor([step_ms, pack_ms, unpack_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms, pack_ms, unpack_ms = [float(x) for x in t.tolist()]
+    assert torch.equal(out, values)
+
+    value_bytes = n * esz
+    value = world * 2 * value_bytes / (step_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    pack_bytes = value_bytes + packed_len
+    unpack_bytes = packed_len + value_bytes
+    pack_gbs = pack_bytes / (pack_ms * 1e-3) / 1e9
+    unpack_gbs = unpack_bytes / (unpack_ms * 1e-3) / 1e9
+    traffic = profiled_traffic()
+    dom = "pack" if pack_ms >= unpack_ms else "unpack"
+    dom_achieved = pack_gbs if dom == "pack" else unpack_gbs
+    dom_traffic = traffic.get(dom)
+    roofline = {"bound": "hbm", "achieved": dom_achieved, "peak": peak, "unit": "GB/s",
+                "frac": dom_achieved / peak, "traffic": (dom_traffic * n) if dom_traffic else None,
+                "kernel": dom + "_kernel", "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback 6650 GB/s",
+                "algorithmic_bytes": pack_bytes if dom == "pack" else unpack_bytes}
+
+    # end to end through the host-buffer C ABI, pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        h_vals = torch.empty(n * esz, dtype=torch.uint8, pin_memory=True)
+        h_vals.copy_(values.view(torch.uint8))
+        h_out = torch.empty(n * esz, dtype=torch.uint8, pin_memory=True)
+        h_packed = torch.empty(packed_len + 4096, dtype=torch.uint8, pin_memory=True)
+        nb = codec.n_blocks
+        h_bo = np.zeros(nb + 1, dtype=np.uint64)
+        h_vo = np.ascontiguousarray(vo, dtype=np.uint64)
+        ns = len(vo) - 1
+        olen = C.c_size_t(0)
+        pk = L.utl_pack_streams_u64 if is64 else L.utl_pack_streams_u32
+        up = L.utl_unpack_streams_u64 if is64 else L.utl_unpack_streams_u32
+        P64 = C.POINTER(C.c_uint64)
+
+        def e2e_step():
+            rc = pk(flag, C.c_void_p(h_vals.data_ptr()), h_vo.ctypes.data_as(P64), ns, C.c_void_p(h_packed.data_ptr()),
+                    h_packed.numel(), h_bo.ctypes.data_as(P64), None, C.byref(olen))
+            assert rc == 0, rc
+            rc = up(C.c_void_p(h_packed.data_ptr()), olen.value, h_bo.ctypes.data_as(P64), h_vo.ctypes.data_as(P64), ns,
+                    C.c_void_p(h_out.data_ptr()))
+            assert rc == 0, rc
+
+        e2e_step()
+        assert torch.equal(h_out, h_vals), "e2e round trip mismatch"
+        e_steps = max(3, min(args.steps, 5))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            e2e_step()
+        e2e_s = (time.perf_counter() - t0) / e_steps
+        if world > 1:
+            t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        meta = 8 * (ns + 1)
+        h2d = value_bytes + meta + packed_len + 8 * (nb + 1) + meta
+        d2h = 8 * (nb + 1) + packed_len + value_bytes + 8
+        e2e = {"value": world * 2 * value_bytes / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
+               "timing": "host wall clock around synchronous C-ABI calls (pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu and args.workload.startswith("c3"):
+        threads = host_threads()
+        S = 1 << 24
+        sample = values[:S].cpu().numpy().view(np.uint32).copy()
+        svo = np.array([0, S], dtype=np.uint64)
+        times = cpu_round_trip(sample, svo, flag, threads)
+        t = sum(times) / len(times)
+        cpu = {"value": 2 * 4 * S / t / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+               "sample": "first %d values (%d MiB) of this workload, %d rounds" % (S, 4 * S >> 20, len(times))}
+
+    if rank == 0:
+        line = {
+            "metric": "round-trip uncompressed GB/s (batched PackUint32 + UnpackUint32)",
+            "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64" if is64 else "u32", "data": "synthetic (seeded on device)",
+            "config": {"workload": wl["desc"], "flag": flag, "values_per_gpu": n, "blocks_per_gpu": codec.n_blocks,
+                       "packed_bytes_per_gpu": packed_len, "bytes_per_value": packed_len / n,
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": "replicas" if world > 1 else "1 GPU"},
+            "pack": {"ms": pack_ms, "uncompressed_GBps": value_bytes / (pack_ms * 1e-3) / 1e9,
+                     "hbm_GBps": pack_gbs, "hbm_frac": pack_gbs / peak},
+            "unpack": {"ms": unpack_ms, "uncompressed_GBps": value_bytes / (unpack_ms * 1e-3) / 1e9,
+                       "hbm_GBps": unpack_gbs, "hbm_frac": unpack_gbs / peak},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

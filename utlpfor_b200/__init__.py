@@ -247,4 +247,5 @@ def NewUint64():
     return Compressor64()
 
 
-from .batch import PackedBatch, plan, pack_batch, unpack_batch, get_batch, pack_streams, unpack_streams  # noqa: E402
+from .batch import (BatchCodec, PackedBatch, get_batch, pack_batch, pack_streams, plan,  # noqa: E402
+                    unpack_batch, unpack_streams)

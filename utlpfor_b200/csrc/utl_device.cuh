@@ -118,21 +118,23 @@ struct GlobalBytes {
 // Bit-width selection, select_bitwidth.go:56-121 / chooseBestFromExcCounts.
 // exc[si] = number of values above 2^(4*si)-1; ties keep the wider width.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void choose_best(const int exc[8], int* best_w, int* best_exc) {
-  int max_si = 8;
+__device__ __forceinline__ void choose_best_packed(uint64_t c, int* best_w, int* best_exc) {
+  // byte si of c is exc[si]; counts do not increase with si, so the
+  // non-zero bytes form a prefix and their number is maxStepIdx
+  int max_si = 0;
 #pragma unroll
-  for (int si = 7; si >= 0; si--)
-    if (exc[si] == 0) max_si = si;
+  for (int si = 0; si < 8; si++) max_si += ((c >> (8 * si)) & 0xFF) != 0;
   int bw = max_si * 4, be = 0;
   int best = 4 + (max_si << 6);
-  // excCostBytesPerValue, select_bitwidth.go:35
-  const uint32_t bpv_lut = 0x44332211u;  // nibble d-1 holds the LUT entry of step delta d
-  for (int si = max_si - 1; si >= 0; si--) {
-    int e = exc[si];
-    int delta = max_si - si;
-    int bpv = (int)((bpv_lut >> (4 * (delta - 1))) & 0xF);
-    int cost = 4 + (si << 6) + 2 + min(e, 16) + ((e + 3) >> 2) + e * bpv;
-    if (cost < best) {
+  // excCostBytesPerValue, select_bitwidth.go:35: nibble d-1 holds the entry of step delta d
+  const uint32_t bpv_lut = 0x44332211u;
+#pragma unroll
+  for (int si = 7; si >= 0; si--) {
+    const int e = (int)((c >> (8 * si)) & 0xFF);
+    const int delta = max_si - si;
+    const int bpv = (int)((bpv_lut >> ((4 * (delta - 1)) & 31)) & 0xF);
+    const int cost = 4 + (si << 6) + 2 + min(e, 16) + ((e + 3) >> 2) + e * bpv;
+    if (si < max_si && cost < best) {
       best = cost;
       bw = si * 4;
       be = e;
@@ -140,6 +142,13 @@ __device__ __forceinline__ void choose_best(const int exc[8], int* best_w, int* 
   }
   *best_w = bw;
   *best_exc = be;
+}
+
+__device__ __forceinline__ void choose_best(const int exc[8], int* best_w, int* best_exc) {
+  uint64_t c = 0;
+#pragma unroll
+  for (int si = 0; si < 8; si++) c |= (uint64_t)(exc[si] & 0xFF) << (8 * si);
+  choose_best_packed(c, best_w, best_exc);
 }
 
 // Warp-wide exception counts at the eight step thresholds.  Each value adds

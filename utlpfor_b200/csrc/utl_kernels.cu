@@ -17,6 +17,7 @@
 
 #include "utl_device.cuh"
 #include "utl_launch.h"
+#include "utl_quad.cuh"
 
 namespace utl {
 
@@ -173,40 +174,67 @@ __global__ void stream_off_kernel(const uint64_t* __restrict__ block_off, const 
 // counter, so every predecessor of a waiting tile is already running.
 constexpr uint32_t kSpinLimit = 1u << 22;
 
-__device__ uint64_t tile_lookback(uint64_t* status, int64_t tile, uint64_t agg, int lane, uint32_t* err) {
-  if (tile == 0) {
-    if (lane == 0) st_relaxed_u64(&status[0], (agg << 2) | 2u);
-    return 0;
-  }
-  if (lane == 0) st_relaxed_u64(&status[tile], (agg << 2) | 1u);
+// Each lane inspects 8 consecutive predecessors per round (lane 0 the 8
+// nearest), so one round covers 256 tiles: with hundreds of tiles in flight
+// the nearest inclusive prefix is normally found in one or two rounds.
+constexpr int kLookPerLane = 8;
+
+// Publish a tile's aggregate (tile 0 publishes its inclusive prefix).
+__device__ __forceinline__ void tile_publish(uint64_t* status, int64_t tile, uint64_t agg) {
+  st_relaxed_u64(&status[tile], (agg << 2) | (tile == 0 ? 2u : 1u));
+}
+
+// Exclusive prefix of a tile whose aggregate is already published; then
+// publishes the tile's inclusive prefix.  Whole warp.
+__device__ uint64_t tile_resolve(uint64_t* status, int64_t tile, uint64_t agg, int lane, uint32_t* err) {
+  if (tile == 0) return 0;
   uint64_t excl = 0;
   int64_t j = tile - 1;
   bool timed_out = false;
   for (;;) {
-    const int64_t idx = j - lane;
-    uint64_t s = 2u;  // before tile 0: an inclusive prefix of zero
-    if (idx >= 0) {
+    uint64_t st[kLookPerLane];
+#pragma unroll
+    for (int i = 0; i < kLookPerLane; i++) {
+      const int64_t idx = j - (int64_t)lane * kLookPerLane - i;
+      st[i] = idx >= 0 ? ld_relaxed_u64(&status[idx]) : 2u;  // before tile 0: prefix 0
+    }
+#pragma unroll
+    for (int i = 0; i < kLookPerLane; i++) {
+      const int64_t idx = j - (int64_t)lane * kLookPerLane - i;
       uint32_t it = 0;
-      s = ld_relaxed_u64(&status[idx]);
-      while ((s & 3u) == 0) {
+      while ((st[i] & 3u) == 0) {
         if (++it > kSpinLimit) {
           timed_out = true;
-          s = 2u;
+          st[i] = 2u;
           break;
         }
         __nanosleep(64);
-        s = ld_relaxed_u64(&status[idx]);
+        st[i] = ld_relaxed_u64(&status[idx]);
       }
     }
-    const unsigned pm = __ballot_sync(kFull, (s & 3u) == 2u);
+    // this lane's nearest inclusive prefix (index into st), or none
+    int fi = kLookPerLane;
+#pragma unroll
+    for (int i = kLookPerLane - 1; i >= 0; i--)
+      if ((st[i] & 3u) == 2u) fi = i;
+    uint64_t part = 0;
+#pragma unroll
+    for (int i = 0; i < kLookPerLane; i++)
+      if (i <= fi) part += st[i] >> 2;
+    const unsigned pm = __ballot_sync(kFull, fi < kLookPerLane);
     const int first = pm ? __ffs(pm) - 1 : 32;
-    excl += warp_sum_u64(lane <= first ? (s >> 2) : 0ull);
+    excl += warp_sum_u64(lane <= first ? part : 0ull);
     if (pm) break;
-    j -= 32;
+    j -= 32 * kLookPerLane;
   }
   if (__any_sync(kFull, timed_out) && lane == 0 && err) atomicOr(err, 1u << 10);
   if (lane == 0) st_relaxed_u64(&status[tile], ((excl + agg) << 2) | 2u);
   return excl;
+}
+
+__device__ uint64_t tile_lookback(uint64_t* status, int64_t tile, uint64_t agg, int lane, uint32_t* err) {
+  if (lane == 0) tile_publish(status, tile, agg);
+  return tile_resolve(status, tile, agg, lane, err);
 }
 
 template <bool U64>
@@ -375,6 +403,223 @@ __global__ void __launch_bounds__(kThreads) unpack_kernel(UnpackArgs a) {
     if (lane == 0) {
       if (a.block_status) a.block_status[b] = status | (ovf << 8);
       if (status != kOK && a.err) atomicOr(a.err, 1u << status);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// quad-per-block batched kernels (uint32): a warp codes 8 blocks at once
+// ------------------------------------------------------------------------
+constexpr int kQWarps = 4;                 // warps per CTA
+constexpr int kQTile = kQWarps * 8;        // blocks per CTA tile
+constexpr int kQThreads = kQWarps * 32;
+constexpr int kQStage = 8 * 528;           // per-warp staging budget (8 blocks up to 528 B)
+constexpr int kQStagePad = 128;            // readable slack past the staged bytes
+constexpr int kQImage = kQTile * 288;      // pack tile image budget
+
+struct QuadUnpackSmem {
+  uint4 stage[kQWarps][(kQStage + kQStagePad) / 16];
+  uint4 patch[kQWarps][8][kBlock / 4];
+};
+
+__global__ void __launch_bounds__(kQThreads) unpack_quad_kernel(UnpackArgs a) {
+  extern __shared__ uint4 smem4[];
+  QuadUnpackSmem& S = *(QuadUnpackSmem*)smem4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int q = lane >> 2, j = lane & 3;
+  const unsigned qm = quad::quad_mask(lane);
+  const int64_t b0 = ((int64_t)blockIdx.x * kQWarps + warp) * 8;
+  if (b0 >= a.n_blocks) return;
+  const int nb = (int)min((int64_t)8, a.n_blocks - b0);
+  // block offsets of the warp's 8 blocks
+  const uint64_t my_off = lane <= nb ? a.block_off[b0 + lane] : 0ull;
+  const uint64_t off0 = __shfl_sync(kFull, my_off, 0);
+  const uint64_t off1 = __shfl_sync(kFull, my_off, nb);
+  const uint64_t next_off = __shfl_down_sync(kFull, my_off, 1);
+  const bool ok = lane >= nb ||
+                  (next_off >= my_off && next_off - my_off <= (uint64_t)kMaxBlock32 && next_off <= a.packed_len);
+  const bool all_ok = __all_sync(kFull, ok);
+  // this quad's block bounds (read by every lane before quads diverge)
+  const uint64_t s = __shfl_sync(kFull, my_off, q), e = __shfl_sync(kFull, my_off, q + 1);
+  const uintptr_t gbase = (uintptr_t)a.packed;
+  const int ph = (int)((gbase + off0) & 15);
+  const bool staged = all_ok && (int64_t)(off1 - off0) + ph + 16 <= kQStage;
+  if (staged) stage_bytes(S.stage[warp], a.packed, a.packed_len, off0, off1, lane, 32);
+  __syncwarp();
+  if (q >= nb) return;
+  const int64_t b = b0 + q;
+  uint64_t first;
+  int want;
+  block_span(a.val_off, a.block_start, a.n_streams, b, &first, &want);
+  int status = kOK, ovf = 0;
+  if (e < s || e - s > (uint64_t)kMaxBlock32 || e > a.packed_len) {
+    status = kErrCountMismatch;
+  } else {
+    const int len = (int)(e - s);
+    uint32_t x[8][4];
+    uint32_t* patch = (uint32_t*)S.patch[warp][q];
+    quad::QResult r;
+    if (staged) {
+      r = quad::quad_unpack_block(SmemBytes{(const uint32_t*)S.stage[warp]}, ph + (int64_t)(s - off0), len, false, x,
+                                  patch, j, qm);
+    } else {
+      r = quad::quad_unpack_block(GlobalBytes{a.packed + s, len}, 0, len, false, x, patch, j, qm);
+    }
+    if (r.status == kOK && (r.count != want || r.consumed != len)) r.status = kErrCountMismatch;
+    if (r.status == kOK) {
+      uint32_t* op = (uint32_t*)a.values + first;
+      if (want == kBlock && ((uintptr_t)op & 15) == 0) {
+#pragma unroll
+        for (int v = 0; v < 8; v++) __stcs((uint4*)(op + 16 * v + 4 * j), make_uint4(x[v][0], x[v][1], x[v][2], x[v][3]));
+      } else {
+#pragma unroll
+        for (int v = 0; v < 8; v++)
+#pragma unroll
+          for (int k = 0; k < 4; k++)
+            if (16 * v + 4 * j + k < want) op[16 * v + 4 * j + k] = x[v][k];
+      }
+    }
+    status = r.status;
+    ovf = r.ovf;
+  }
+  if (j == 0) {
+    if (a.block_status) a.block_status[b] = status | (ovf << 8);
+    if (status != kOK && a.err) atomicOr(a.err, 1u << status);
+  }
+}
+
+struct QuadPackSmem {
+  uint32_t hb[kQTile][kBlock];
+  uint8_t idx[kQTile][16];
+  uint4 image[2][kQImage / 16 + 2];
+  int len[kQTile];
+  int off[kQTile + 1];
+  int64_t next;
+  uint64_t prefix;
+};
+
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Pack: per tile of kQTile blocks, (A) every quad plans its block; warp 0
+// scans the lengths and publishes the tile's aggregate at once; (C) every
+// quad writes its bytes into the tile image; warp 0 then resolves the
+// tile's byte offset by look-back (its predecessors have had phase C to
+// publish) and (D) every warp streams its part of the image to HBM,
+// shifted to the destination's alignment, with aligned 16-byte stores.
+// Tiles are taken from the work counter just before their phase A, so a
+// tile's predecessors are always at least as far along; images alternate
+// between tiles.  Tiles too large for the image are written in phase D
+// straight to HBM.
+__global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
+  extern __shared__ uint4 smem4[];
+  QuadPackSmem& S = *(QuadPackSmem*)smem4;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int q = lane >> 2, j = lane & 3;
+  const unsigned qm = quad::quad_mask(lane);
+  const int lb = warp * 8 + q;  // block within the tile
+
+  for (int it = 0;; it++) {
+    if (tid == 0) S.next = (int64_t)atomicAdd((unsigned long long*)a.counter, 1ull);
+    __syncthreads();
+    const int64_t tile = S.next;
+    if (tile >= a.n_tiles) break;
+    const int64_t b = tile * kQTile + lb;
+    const bool live = b < a.n_blocks;
+
+    // phase A: decisions and lengths
+    uint32_t x[8][4];
+    quad::QPlan plan;
+    plan.len = 0;
+    if (live) {
+      uint64_t first;
+      int n;
+      block_span(a.val_off, a.block_start, a.n_streams, b, &first, &n);
+      const uint32_t* vp = (const uint32_t*)a.values + first;
+      if (n == kBlock && ((uintptr_t)vp & 15) == 0) {
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+          const uint4 t = __ldcs((const uint4*)(vp + 16 * v + 4 * j));
+          x[v][0] = t.x; x[v][1] = t.y; x[v][2] = t.z; x[v][3] = t.w;
+        }
+        plan = quad::quad_plan_block<true>(x, n, a.flag, kTypeU32, kModePlain, S.hb[lb], S.idx[lb], j, qm);
+      } else {
+#pragma unroll
+        for (int v = 0; v < 8; v++)
+#pragma unroll
+          for (int k = 0; k < 4; k++) x[v][k] = (16 * v + 4 * j + k < n) ? __ldcs(vp + 16 * v + 4 * j + k) : 0u;
+        plan = quad::quad_plan_block<false>(x, n, a.flag, kTypeU32, kModePlain, S.hb[lb], S.idx[lb], j, qm);
+      }
+    }
+    if (j == 0) S.len[lb] = plan.len;
+    __syncthreads();
+
+    // tile scan; the aggregate goes out immediately
+    if (warp == 0) {
+      const int l = S.len[lane];
+      const int incl = warp_incl_scan(l, lane);
+      S.off[lane] = incl - l;
+      if (lane == 31) {
+        S.off[kQTile] = incl;
+        tile_publish(a.tile_status, tile, (uint64_t)incl);
+      }
+    }
+    __syncthreads();
+    const int total = S.off[kQTile];
+    const bool use_image = total <= kQImage;
+    uint4* img4 = S.image[it & 1];
+    uint8_t* img = (uint8_t*)img4;
+
+    // phase C: bytes of each block into the image
+    if (live && use_image)
+      quad::quad_write_block(plan, x, kModePlain, 0, S.hb[lb], S.idx[lb], img + S.off[lb], j, qm);
+
+    // look-back for the tile's byte offset
+    if (warp == 0) {
+      const uint64_t prefix = tile_resolve(a.tile_status, tile, (uint64_t)total, lane, a.err);
+      if (lane == 0) S.prefix = prefix;
+    }
+    __syncthreads();
+    const uint64_t G = S.prefix;
+    const bool fits = G + (uint64_t)total <= a.out_cap;
+    if (!fits && tid == 0 && a.err) atomicOr(a.err, 1u << 9);
+    if (live && j == 0) {
+      const uint64_t g = G + (uint64_t)S.off[lb];
+      a.block_off[b] = g;
+      if (b == a.n_blocks - 1) a.block_off[a.n_blocks] = g + (uint64_t)plan.len;
+    }
+    if (!fits) continue;
+    if (!use_image) {
+      if (live) quad::quad_write_block(plan, x, kModePlain, 0, S.hb[lb], S.idx[lb], a.out + G + S.off[lb], j, qm);
+      continue;
+    }
+
+    // phase D: this warp's image bytes [off[8w], off[8w+8]) go to
+    // out[G + r] in aligned 16-byte chunks assembled with funnel shifts;
+    // partial chunks at the two ends are shared with neighbours and are
+    // written bytewise
+    const int r0 = S.off[warp * 8], r1 = S.off[warp * 8 + 8];
+    if (r1 > r0) {
+      const uint64_t A0 = (uint64_t)(uintptr_t)a.out + G;     // address of image byte 0
+      const uint64_t c0 = (A0 + (uint64_t)r0) >> 4, c1 = (A0 + (uint64_t)r1 + 15) >> 4;
+      const int shift_b = (int)((16 - (A0 & 15)) & 15);      // image offset of an aligned chunk, mod 16
+      const uint32_t* iw = (const uint32_t*)img4;
+      for (uint64_t c = c0 + lane; c < c1; c += 32) {
+        const int64_t o = (int64_t)(c * 16 - A0);           // image offset of this chunk
+        uint8_t* gp = (uint8_t*)(uintptr_t)(c * 16);
+        if (o >= r0 && o + 16 <= r1) {
+          const int wq = (int)(o >> 2), sh = (shift_b & 3) * 8;
+          const uint32_t w0 = iw[wq], w1 = iw[wq + 1], w2 = iw[wq + 2], w3 = iw[wq + 3], w4 = iw[wq + 4];
+          __stcs((uint4*)gp, make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh),
+                                        __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh)));
+        } else {
+          for (int bb = 0; bb < 16; bb++) {
+            const int64_t io = o + bb;
+            if (io >= r0 && io < r1) gp[bb] = img[io];
+          }
+        }
+      }
     }
   }
 }
@@ -703,7 +948,29 @@ cudaError_t stream_offsets(const uint64_t* block_off, const uint64_t* bstart, in
   return cudaGetLastError();
 }
 
-cudaError_t pack(bool u64, const PackArgs& a, cudaStream_t st) {
+static int g_quad_pack_ctas = 0;
+static bool g_quad_unpack_cfg = false;
+
+cudaError_t pack(bool u64, const PackArgs& a_in, cudaStream_t st) {
+  if (!u64) {
+    PackArgs a = a_in;
+    a.n_tiles = (a.n_blocks + kQTile - 1) / kQTile;
+    const size_t smem = sizeof(QuadPackSmem);
+    if (g_quad_pack_ctas == 0) {
+      cudaError_t e = cudaFuncSetAttribute(pack_quad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      cudaFuncSetAttribute(pack_quad_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_quad_pack_ctas, pack_quad_kernel, kQThreads, smem);
+      if (g_quad_pack_ctas <= 0) g_quad_pack_ctas = 1;
+    }
+    int64_t grid = (int64_t)num_sms() * g_quad_pack_ctas;
+    if (grid > a.n_tiles) grid = a.n_tiles;
+    if (grid < 1) grid = 1;
+    pack_quad_kernel<<<(unsigned)grid, kQThreads, smem, st>>>(a);
+    note_launch(1);
+    return cudaGetLastError();
+  }
+  const PackArgs& a = a_in;
   const size_t smem = pack_smem(u64);
   const int idx = u64 ? 1 : 0;
   if (g_pack_ctas_per_sm[idx] == 0) {
@@ -729,6 +996,20 @@ cudaError_t pack(bool u64, const PackArgs& a, cudaStream_t st) {
 }
 
 cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
+  if (!u64) {
+    const size_t smem = sizeof(QuadUnpackSmem);
+    if (!g_quad_unpack_cfg) {
+      cudaError_t e = cudaFuncSetAttribute(unpack_quad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      cudaFuncSetAttribute(unpack_quad_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+      g_quad_unpack_cfg = true;
+    }
+    const int64_t grid = (a.n_blocks + kQTile - 1) / kQTile;
+    if (grid <= 0) return cudaSuccess;
+    unpack_quad_kernel<<<(unsigned)grid, kQThreads, smem, st>>>(a);
+    note_launch(1);
+    return cudaGetLastError();
+  }
   const size_t smem = unpack_smem(u64);
   static bool configured[2] = {false, false};
   const int idx = u64 ? 1 : 0;
