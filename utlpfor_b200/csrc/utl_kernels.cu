@@ -52,6 +52,11 @@ __device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
   asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+__device__ __forceinline__ uint64_t shfl_up64(uint64_t v, int d) {
+  const uint32_t lo = __shfl_up_sync(kFull, (uint32_t)v, d), hi = __shfl_up_sync(kFull, (uint32_t)(v >> 32), d);
+  return ((uint64_t)hi << 32) | lo;
+}
+
 __device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) v += shfl_xor64(v, d);
@@ -213,6 +218,68 @@ __device__ uint64_t tile_resolve(uint64_t* status, int64_t tile, uint64_t agg, i
       }
     }
     // this lane's nearest inclusive prefix (index into st), or none
+    int fi = kLookPerLane;
+#pragma unroll
+    for (int i = kLookPerLane - 1; i >= 0; i--)
+      if ((st[i] & 3u) == 2u) fi = i;
+    uint64_t part = 0;
+#pragma unroll
+    for (int i = 0; i < kLookPerLane; i++)
+      if (i <= fi) part += st[i] >> 2;
+    const unsigned pm = __ballot_sync(kFull, fi < kLookPerLane);
+    const int first = pm ? __ffs(pm) - 1 : 32;
+    excl += warp_sum_u64(lane <= first ? part : 0ull);
+    if (pm) break;
+    j -= 32 * kLookPerLane;
+  }
+  if (__any_sync(kFull, timed_out) && lane == 0 && err) atomicOr(err, 1u << 10);
+  if (lane == 0) st_relaxed_u64(&status[tile], ((excl + agg) << 2) | 2u);
+  return excl;
+}
+
+// The first round of a look-back, issued early: the loads complete in the
+// background while the caller does other work.
+struct LookRound {
+  uint64_t st[kLookPerLane];
+};
+__device__ __forceinline__ void tile_resolve_issue(const uint64_t* status, int64_t tile, int lane, LookRound& r) {
+#pragma unroll
+  for (int i = 0; i < kLookPerLane; i++) {
+    const int64_t idx = tile - 1 - (int64_t)lane * kLookPerLane - i;
+    r.st[i] = (tile > 0 && idx >= 0) ? ld_relaxed_u64(&status[idx]) : 2u;
+  }
+}
+// Finish the look-back started by tile_resolve_issue (whole warp) and
+// publish the tile's inclusive prefix.
+__device__ uint64_t tile_resolve_finish(uint64_t* status, int64_t tile, uint64_t agg, int lane, uint32_t* err,
+                                        LookRound& r) {
+  if (tile == 0) return 0;
+  uint64_t excl = 0;
+  int64_t j = tile - 1;
+  bool timed_out = false;
+  bool first_round = true;
+  for (;;) {
+    uint64_t st[kLookPerLane];
+#pragma unroll
+    for (int i = 0; i < kLookPerLane; i++) {
+      const int64_t idx = j - (int64_t)lane * kLookPerLane - i;
+      st[i] = first_round ? r.st[i] : (idx >= 0 ? ld_relaxed_u64(&status[idx]) : 2u);
+    }
+    first_round = false;
+#pragma unroll
+    for (int i = 0; i < kLookPerLane; i++) {
+      const int64_t idx = j - (int64_t)lane * kLookPerLane - i;
+      uint32_t it = 0;
+      while ((st[i] & 3u) == 0) {
+        if (++it > kSpinLimit) {
+          timed_out = true;
+          st[i] = 2u;
+          break;
+        }
+        __nanosleep(64);
+        st[i] = ld_relaxed_u64(&status[idx]);
+      }
+    }
     int fi = kLookPerLane;
 #pragma unroll
     for (int i = kLookPerLane - 1; i >= 0; i--)
@@ -492,26 +559,51 @@ struct QuadPackSmem {
   uint32_t hb[kQTile][kBlock];
   uint8_t idx[kQTile][16];
   uint4 image[2][kQImage / 16 + 2];
-  int len[kQTile];
-  int off[kQTile + 1];
-  int64_t next;
+  int len[2][kQTile];
+  int off[2][kQTile + 1];
+  int64_t tile[2];
   uint64_t prefix;
+  int64_t next;
 };
 
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+// Phase D of a tile whose image is complete and whose byte offset G is
+// known: this warp's image bytes [r0, r1) go to out[G + r] in aligned
+// 16-byte chunks assembled with funnel shifts; partial chunks at the two
+// ends are shared with neighbours and written bytewise.
+__device__ __forceinline__ void image_copy_out(const uint4* img4, int r0, int r1, uint8_t* out, uint64_t G, int lane) {
+  if (r1 <= r0) return;
+  const uint8_t* img = (const uint8_t*)img4;
+  const uint64_t A0 = (uint64_t)(uintptr_t)out + G;  // address of image byte 0
+  const uint64_t c0 = (A0 + (uint64_t)r0) >> 4, c1 = (A0 + (uint64_t)r1 + 15) >> 4;
+  const int sh = (int)((16 - (A0 & 15)) & 3) * 8;
+  const uint32_t* iw = (const uint32_t*)img4;
+  for (uint64_t c = c0 + lane; c < c1; c += 32) {
+    const int64_t o = (int64_t)(c * 16 - A0);  // image offset of this chunk
+    uint8_t* gp = (uint8_t*)(uintptr_t)(c * 16);
+    if (o >= r0 && o + 16 <= r1) {
+      const int wq = (int)(o >> 2);
+      const uint32_t w0 = iw[wq], w1 = iw[wq + 1], w2 = iw[wq + 2], w3 = iw[wq + 3], w4 = iw[wq + 4];
+      __stcs((uint4*)gp, make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh),
+                                    __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh)));
+    } else {
+      for (int bb = 0; bb < 16; bb++) {
+        const int64_t io = o + bb;
+        if (io >= r0 && io < r1) gp[bb] = img[io];
+      }
+    }
+  }
 }
 
-// Pack: per tile of kQTile blocks, (A) every quad plans its block; warp 0
-// scans the lengths and publishes the tile's aggregate at once; (C) every
-// quad writes its bytes into the tile image; warp 0 then resolves the
-// tile's byte offset by look-back (its predecessors have had phase C to
-// publish) and (D) every warp streams its part of the image to HBM,
-// shifted to the destination's alignment, with aligned 16-byte stores.
-// Tiles are taken from the work counter just before their phase A, so a
-// tile's predecessors are always at least as far along; images alternate
-// between tiles.  Tiles too large for the image are written in phase D
-// straight to HBM.
+// Pack, software-pipelined over tiles of kQTile blocks.  Iteration i:
+// take tile t_i; warp 0 issues the look-back loads of t_{i-1}; (A) every
+// quad plans its block of t_i; warp 0 scans t_i's lengths and publishes
+// t_i's aggregate, then finishes t_{i-1}'s look-back (its loads have
+// landed during phase A); (D) every warp streams its part of t_{i-1}'s
+// image to HBM at the resolved offset; (C) every quad writes t_i's bytes
+// into the other image.  Tiles are taken from the work counter just before
+// their phase A, so predecessors are always at least as far along.  A tile
+// too large for the image is resolved and written straight to HBM in its
+// own iteration.
 __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
   extern __shared__ uint4 smem4[];
   QuadPackSmem& S = *(QuadPackSmem*)smem4;
@@ -520,15 +612,20 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
   const unsigned qm = quad::quad_mask(lane);
   const int lb = warp * 8 + q;  // block within the tile
 
+  if (tid == 0) S.tile[1] = -1;  // no pending tile
   for (int it = 0;; it++) {
+    const int cb = it & 1, pb = cb ^ 1;  // buffers of this and the pending tile
     if (tid == 0) S.next = (int64_t)atomicAdd((unsigned long long*)a.counter, 1ull);
     __syncthreads();
-    const int64_t tile = S.next;
-    if (tile >= a.n_tiles) break;
-    const int64_t b = tile * kQTile + lb;
-    const bool live = b < a.n_blocks;
+    const int64_t tile = S.next < a.n_tiles ? S.next : -1;
+    const int64_t ptile = S.tile[pb];
+    if (tid == 0) S.tile[cb] = tile;
+    LookRound lr;
+    if (warp == 0 && ptile >= 0) tile_resolve_issue(a.tile_status, ptile, lane, lr);
 
-    // phase A: decisions and lengths
+    // phase A: decisions and lengths of tile t_i
+    const int64_t b = tile * kQTile + lb;
+    const bool live = tile >= 0 && b < a.n_blocks;
     uint32_t x[8][4];
     quad::QPlan plan;
     plan.len = 0;
@@ -552,73 +649,73 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
         plan = quad::quad_plan_block<false>(x, n, a.flag, kTypeU32, kModePlain, S.hb[lb], S.idx[lb], j, qm);
       }
     }
-    if (j == 0) S.len[lb] = plan.len;
+    if (j == 0) S.len[cb][lb] = plan.len;
     __syncthreads();
+    if (tile < 0 && ptile < 0) break;
 
-    // tile scan; the aggregate goes out immediately
+    // warp 0: scan of t_i and its aggregate first (no tile's publication
+    // ever waits on a look-back), then the look-back of t_{i-1}, whose
+    // loads have landed during phase A
     if (warp == 0) {
-      const int l = S.len[lane];
-      const int incl = warp_incl_scan(l, lane);
-      S.off[lane] = incl - l;
-      if (lane == 31) {
-        S.off[kQTile] = incl;
-        tile_publish(a.tile_status, tile, (uint64_t)incl);
+      if (tile >= 0) {
+        const int l = S.len[cb][lane];
+        const int incl = warp_incl_scan(l, lane);
+        S.off[cb][lane] = incl - l;
+        if (lane == 31) {
+          S.off[cb][kQTile] = incl;
+          tile_publish(a.tile_status, tile, (uint64_t)incl);
+        }
+      }
+      if (ptile >= 0) {
+        const uint64_t pre = tile_resolve_finish(a.tile_status, ptile, (uint64_t)S.off[pb][kQTile], lane, a.err, lr);
+        if (lane == 0) S.prefix = pre;
       }
     }
     __syncthreads();
-    const int total = S.off[kQTile];
-    const bool use_image = total <= kQImage;
-    uint4* img4 = S.image[it & 1];
-    uint8_t* img = (uint8_t*)img4;
 
-    // phase C: bytes of each block into the image
-    if (live && use_image)
-      quad::quad_write_block(plan, x, kModePlain, 0, S.hb[lb], S.idx[lb], img + S.off[lb], j, qm);
-
-    // look-back for the tile's byte offset
-    if (warp == 0) {
-      const uint64_t prefix = tile_resolve(a.tile_status, tile, (uint64_t)total, lane, a.err);
-      if (lane == 0) S.prefix = prefix;
-    }
-    __syncthreads();
-    const uint64_t G = S.prefix;
-    const bool fits = G + (uint64_t)total <= a.out_cap;
-    if (!fits && tid == 0 && a.err) atomicOr(a.err, 1u << 9);
-    if (live && j == 0) {
-      const uint64_t g = G + (uint64_t)S.off[lb];
-      a.block_off[b] = g;
-      if (b == a.n_blocks - 1) a.block_off[a.n_blocks] = g + (uint64_t)plan.len;
-    }
-    if (!fits) continue;
-    if (!use_image) {
-      if (live) quad::quad_write_block(plan, x, kModePlain, 0, S.hb[lb], S.idx[lb], a.out + G + S.off[lb], j, qm);
-      continue;
+    // phase D of t_{i-1}
+    if (ptile >= 0) {
+      const uint64_t G = S.prefix;
+      const int ptotal = S.off[pb][kQTile];
+      const bool fits = G + (uint64_t)ptotal <= a.out_cap;
+      const int64_t pbk = ptile * kQTile + lb;
+      if (pbk < a.n_blocks && j == 0) {
+        const uint64_t g = G + (uint64_t)S.off[pb][lb];
+        a.block_off[pbk] = g;
+        if (pbk == a.n_blocks - 1) a.block_off[a.n_blocks] = g + (uint64_t)S.len[pb][lb];
+      }
+      if (fits) image_copy_out(S.image[pb], S.off[pb][warp * 8], S.off[pb][warp * 8 + 8], a.out, G, lane);
+      else if (tid == 0 && a.err) atomicOr(a.err, 1u << 9);
     }
 
-    // phase D: this warp's image bytes [off[8w], off[8w+8]) go to
-    // out[G + r] in aligned 16-byte chunks assembled with funnel shifts;
-    // partial chunks at the two ends are shared with neighbours and are
-    // written bytewise
-    const int r0 = S.off[warp * 8], r1 = S.off[warp * 8 + 8];
-    if (r1 > r0) {
-      const uint64_t A0 = (uint64_t)(uintptr_t)a.out + G;     // address of image byte 0
-      const uint64_t c0 = (A0 + (uint64_t)r0) >> 4, c1 = (A0 + (uint64_t)r1 + 15) >> 4;
-      const int shift_b = (int)((16 - (A0 & 15)) & 15);      // image offset of an aligned chunk, mod 16
-      const uint32_t* iw = (const uint32_t*)img4;
-      for (uint64_t c = c0 + lane; c < c1; c += 32) {
-        const int64_t o = (int64_t)(c * 16 - A0);           // image offset of this chunk
-        uint8_t* gp = (uint8_t*)(uintptr_t)(c * 16);
-        if (o >= r0 && o + 16 <= r1) {
-          const int wq = (int)(o >> 2), sh = (shift_b & 3) * 8;
-          const uint32_t w0 = iw[wq], w1 = iw[wq + 1], w2 = iw[wq + 2], w3 = iw[wq + 3], w4 = iw[wq + 4];
-          __stcs((uint4*)gp, make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh),
-                                        __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh)));
-        } else {
-          for (int bb = 0; bb < 16; bb++) {
-            const int64_t io = o + bb;
-            if (io >= r0 && io < r1) gp[bb] = img[io];
-          }
+    // phase C of t_i
+    if (tile >= 0) {
+      const int total = S.off[cb][kQTile];
+      if (total <= kQImage) {
+        if (live)
+          quad::quad_write_block(plan, x, kModePlain, 0, S.hb[lb], S.idx[lb], (uint8_t*)S.image[cb] + S.off[cb][lb],
+                                 j, qm);
+      } else {
+        // too large for the image: resolve now and write straight to HBM
+        __syncthreads();
+        if (warp == 0) {
+          LookRound r2;
+          tile_resolve_issue(a.tile_status, tile, lane, r2);
+          const uint64_t pre = tile_resolve_finish(a.tile_status, tile, (uint64_t)total, lane, a.err, r2);
+          if (lane == 0) S.prefix = pre;
         }
+        __syncthreads();
+        const uint64_t G = S.prefix;
+        const bool fits = G + (uint64_t)total <= a.out_cap;
+        if (live && j == 0) {
+          const uint64_t g = G + (uint64_t)S.off[cb][lb];
+          a.block_off[b] = g;
+          if (b == a.n_blocks - 1) a.block_off[a.n_blocks] = g + (uint64_t)plan.len;
+        }
+        if (fits && live)
+          quad::quad_write_block(plan, x, kModePlain, 0, S.hb[lb], S.idx[lb], a.out + G + S.off[cb][lb], j, qm);
+        if (!fits && tid == 0 && a.err) atomicOr(a.err, 1u << 9);
+        if (tid == 0) S.tile[cb] = -1;  // nothing pending
       }
     }
   }
