@@ -173,10 +173,14 @@ class ClockSampler:
 
 
 def gpu_smi_id(torch, dev_index):
+    """nvidia-smi -i id of a torch device: its UUID, else its PCI bus id."""
     try:
-        bus = torch.cuda.get_device_properties(dev_index).pci_bus_id
-        if bus:
-            return bus
+        props = torch.cuda.get_device_properties(dev_index)
+        u = getattr(props, "uuid", None)
+        if u:
+            u = str(u)
+            return u if u.startswith("GPU-") else "GPU-" + u
+        return "%08X:%02X:%02X.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
     except Exception:
         pass
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")

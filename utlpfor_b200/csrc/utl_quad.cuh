@@ -59,30 +59,6 @@ __device__ __forceinline__ uint64_t shr64_clamp(uint64_t x, uint32_t s) {
 // Sum of the 2-bit fields of x.
 __device__ __forceinline__ int sum2bit(uint32_t x) { return __popc(x & 0x55555555u) + 2 * __popc(x & 0xAAAAAAAAu); }
 
-// Byte counters of the eight step thresholds for one value: byte si is 1
-// when len(x) > 4*si (the value is an exception at step width 4*si).
-__device__ __forceinline__ uint64_t bin_counts(uint32_t x) {
-  const uint32_t bin = (uint32_t)(35 - __clz(x)) >> 2;
-  return shr64_clamp(0x0101010101010101ull, 64u - 8u * bin);
-}
-
-// Quad-wide exc[si] (byte si) of select_bitwidth.go:41-51 from per-thread
-// counters; a byte cannot carry (at most 128 per byte).
-__device__ __forceinline__ uint64_t quad_exc(uint64_t c, unsigned qm) {
-  const uint32_t lo = qsum((uint32_t)c, qm), hi = qsum((uint32_t)(c >> 32), qm);
-  return ((uint64_t)hi << 32) | lo;
-}
-
-__device__ __forceinline__ uint64_t thread_counts(const uint32_t (&x)[8][4], const bool (&valid)[8][4]) {
-  uint64_t c = 0;
-#pragma unroll
-  for (int v = 0; v < 8; v++)
-#pragma unroll
-    for (int k = 0; k < 4; k++)
-      if (valid[v][k]) c += bin_counts(x[v][k]);
-  return c;
-}
-
 // ---------------------------------------------------------------- unpack
 struct QResult {
   int status;
@@ -354,47 +330,39 @@ __device__ __forceinline__ uint32_t shl_clamp(uint32_t x, uint32_t s) {
   return r;
 }
 
-// Per-thread histogram of step bins 1..8 in byte lanes: lo holds bins 1-4,
-// hi bins 5-8 (bin = ceil(len/4), select_bitwidth.go:46).  The shift
-// amount (62 - 2*clz) & ~7 equals 8*(bin-1); out-of-range amounts clamp to
-// zero.
+// Per-thread histogram of the values' leading-zero buckets b = clz/4
+// (b = 8 - bin, bin = ceil(len/4) of select_bitwidth.go:46; zero values
+// fall in bucket 8 and are dropped by the clamped shift).  Each value adds
+// 1 << (clz & ~3) to a word of eight 4-bit counters; the values are split
+// over three words so no counter exceeds 15, then the nibbles are widened
+// to bytes: E holds buckets 0,2,4,6 and O buckets 1,3,5,7.
 template <bool kAll>
-__device__ __forceinline__ void bin_hist(const uint32_t (&x)[8][4], int n, int j, uint32_t& lo, uint32_t& hi) {
-  lo = 0;
-  hi = 0;
+__device__ __forceinline__ void bucket_hist(const uint32_t (&x)[8][4], int n, int j, uint32_t& E, uint32_t& O) {
+  uint32_t acc[3] = {0, 0, 0};
 #pragma unroll
   for (int v = 0; v < 8; v++)
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      const uint32_t t = (uint32_t)(62 - 2 * __clz(x[v][k])) & ~7u;
-      const uint32_t a = shl_clamp(1u, t), b = shl_clamp(1u, t - 32u);
-      if (kAll || 16 * v + 4 * j + k < n) {
-        lo += a;
-        hi += b;
-      }
+      const uint32_t add = shl_clamp(1u, (uint32_t)__clz(x[v][k]) & ~3u);
+      if (kAll || 16 * v + 4 * j + k < n) acc[(4 * v + k) / 11] += add;
     }
+  E = (acc[0] & 0x0F0F0F0Fu) + (acc[1] & 0x0F0F0F0Fu) + (acc[2] & 0x0F0F0F0Fu);
+  O = ((acc[0] >> 4) & 0x0F0F0F0Fu) + ((acc[1] >> 4) & 0x0F0F0F0Fu) + ((acc[2] >> 4) & 0x0F0F0F0Fu);
 }
 
-// exc[si] (byte si) = values with bin > si: suffix sums of the quad's
-// histogram (bin 0 never counts).  Bytes stay below 256 (at most 128).
-__device__ __forceinline__ uint64_t quad_exc_from_hist(uint32_t lo, uint32_t hi, unsigned qm) {
-  lo = qsum(lo, qm);
-  hi = qsum(hi, qm);
-  // byte b of lo is hist[b+1], byte b of hi is hist[b+5]
-  const uint32_t hs = (hi >> 24) + ((hi >> 16) & 0xFF) + ((hi >> 8) & 0xFF) + (hi & 0xFF);
-  uint32_t e_hi = 0, e_lo = 0, acc = 0;
-  // exc[7] = hist[8]; exc[si] = exc[si+1] + hist[si+1]
-#pragma unroll
-  for (int si = 7; si >= 4; si--) {
-    acc += (hi >> (8 * (si - 4))) & 0xFF;
-    e_hi |= acc << (8 * (si - 4));
-  }
-  acc = hs;
-#pragma unroll
-  for (int si = 3; si >= 0; si--) {
-    acc += (lo >> (8 * si)) & 0xFF;
-    e_lo |= acc << (8 * si);
-  }
+// exc[si] (byte si) = values with bin > si = values in buckets < 8 - si:
+// the quad's bucket counts in order, prefix-summed, read back to front.
+// Every byte stays at or below 128.
+__device__ __forceinline__ uint64_t quad_exc_from_buckets(uint32_t E, uint32_t O, unsigned qm) {
+  E = qsum(E, qm);
+  O = qsum(O, qm);
+  const uint32_t b03 = __byte_perm(E, O, 0x5140);  // buckets 0,1,2,3
+  const uint32_t b47 = __byte_perm(E, O, 0x7362);  // buckets 4,5,6,7
+  const uint32_t p03 = b03 * 0x01010101u;          // byte k: buckets 0..k
+  const uint32_t p47 = b47 * 0x01010101u + (p03 >> 24) * 0x01010101u;
+  // exc[si] = prefix byte 7 - si
+  const uint32_t e_lo = __byte_perm(p47, 0, 0x0123);  // si 0..3 <- prefix bytes 7..4
+  const uint32_t e_hi = __byte_perm(p03, 0, 0x0123);  // si 4..7 <- prefix bytes 3..0
   return ((uint64_t)e_hi << 32) | e_lo;
 }
 
@@ -419,7 +387,7 @@ __device__ QPlan quad_plan_block(uint32_t (&x)[8][4], int n, int flag, uint32_t 
   bool use_for = false;
   uint32_t base = 0;
   int fw = 0;
-  uint32_t h_lo = 0, h_hi = 0;
+  uint32_t h_e = 0, h_o = 0;
   bool have_hist = false;
   if (!(flag & kNoFOR)) {
     uint32_t mn = 0xFFFFFFFFu, mx = 0u;
@@ -436,10 +404,10 @@ __device__ QPlan quad_plan_block(uint32_t (&x)[8][4], int n, int flag, uint32_t 
       const int for_max = round_step(len32(mx - mn));
       const int raw_max = round_step(len32(mx));
       if (for_max < raw_max) {
-        bin_hist<kAll>(x, n, j, h_lo, h_hi);
+        bucket_hist<kAll>(x, n, j, h_e, h_o);
         have_hist = true;
         int std_w, dummy;
-        choose_best_packed(quad_exc_from_hist(h_lo, h_hi, qm), &std_w, &dummy);
+        choose_best_packed(quad_exc_from_buckets(h_e, h_o, qm), &std_w, &dummy);
         if (for_max < std_w) {
           use_for = true;
           base = mn;
@@ -488,8 +456,8 @@ __device__ QPlan quad_plan_block(uint32_t (&x)[8][4], int n, int flag, uint32_t 
       for (int k = 0; k < 4; k++) o |= x[v][k];
     bw = round_step(len32(qor(o, qm)));
   } else {
-    if (!have_hist) bin_hist<kAll>(x, n, j, h_lo, h_hi);
-    choose_best_packed(quad_exc_from_hist(h_lo, h_hi, qm), &bw, &exc_n);
+    if (!have_hist) bucket_hist<kAll>(x, n, j, h_e, h_o);
+    choose_best_packed(quad_exc_from_buckets(h_e, h_o, qm), &bw, &exc_n);
   }
   QPlan p;
   p.bw = bw;
