@@ -57,6 +57,7 @@ extern "C" {
 #define UTL_ERR_TIMEOUT 10       /* device wait gave up (never expected) */
 #define UTL_ERR_ARG 11           /* bad argument (NULL, size, alignment) */
 #define UTL_ERR_CUDA 12          /* CUDA runtime error; see utl_last_cuda_error */
+#define UTL_ERR_SCRATCH_LIMIT 13 /* batch too large for the built-in scratch of a _noalloc call */
 
 /* ---- flags (utlpfor.go:24-68) ---- */
 #define UTL_DELTA 1
@@ -167,6 +168,31 @@ UTL_API int utl_pack_batch_u64(uint8_t flag, const uint64_t *d_values,
                        size_t out_cap, uint64_t *d_block_off,
                        uint64_t *d_stream_byte_off, void *d_scratch,
                        size_t scratch_bytes, uint32_t *d_err, void *stream);
+
+/* utl_pack_batch_u32 for callers that cannot allocate device memory while
+ * they pack: work recorded into a CUDA graph (no allocation during stream
+ * capture), latency-bound serving loops that cannot take the device-wide
+ * synchronisation of cudaMalloc/cudaFree, and hosts that own a fixed device
+ * memory budget.  It has no counterpart in the reference (the Go library
+ * never touches device memory).  Same arguments as utl_pack_batch_u32
+ * without the scratch: the look-back tile states live in a 2 MiB array
+ * built into the library, which every GPU that loads the library keeps
+ * until the process exits.  Batches above
+ * utl_pack_batch_u32_noalloc_max_blocks() blocks (about 4.2 million, i.e.
+ * 5.4e8 values) are rejected with UTL_ERR_SCRATCH_LIMIT.  The first call
+ * on a device looks up the array's device address (with that device
+ * current); make that first call before any stream capture.  All calls on
+ * a device share the array, so calls that overlap on the GPU (different
+ * streams, or threads without ordering) race: serialise them.  Allocates
+ * nothing and calls no allocating routine. */
+UTL_API int utl_pack_batch_u32_noalloc(uint8_t flag, const uint32_t *d_values,
+                               const uint64_t *d_val_off,
+                               const uint64_t *d_block_start, int n_streams,
+                               int64_t n_blocks, uint8_t *d_out,
+                               size_t out_cap, uint64_t *d_block_off,
+                               uint64_t *d_stream_byte_off, uint32_t *d_err,
+                               void *stream);
+UTL_API int64_t utl_pack_batch_u32_noalloc_max_blocks(void);
 
 /* Unpack every block.  Block b is d_packed[d_block_off[b] .. d_block_off[b+1])
  * and must decode to the stream table's count, consuming exactly its

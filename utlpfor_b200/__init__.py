@@ -76,7 +76,8 @@ _MSG = {1: "UTLpfor: invalid buffer", 2: "UTLpfor: position out of range",
         3: "UTLpfor: invalid block length", 4: "UTLpfor: invalid header flags",
         5: "UTLpfor: unsupported integer type", 6: "UTLpfor: not implemented",
         8: "block count or length disagrees with the stream table", 9: "output capacity too small",
-        10: "device wait timed out", 11: "invalid argument", 12: "CUDA error"}
+        10: "device wait timed out", 11: "invalid argument", 12: "CUDA error",
+        13: "batch exceeds the built-in scratch of the no-allocation pack"}
 
 
 def _raise(code, ovf=0):

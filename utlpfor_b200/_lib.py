@@ -44,6 +44,9 @@ SIGNATURES = [
                                      C.c_size_t, VP, VP]),
     ("utl_pack_batch_u64", C.c_int, [C.c_uint8, VP, VP, VP, C.c_int, C.c_int64, VP, C.c_size_t, VP, VP, VP,
                                      C.c_size_t, VP, VP]),
+    ("utl_pack_batch_u32_noalloc", C.c_int, [C.c_uint8, VP, VP, VP, C.c_int, C.c_int64, VP, C.c_size_t, VP, VP, VP,
+                                             VP]),
+    ("utl_pack_batch_u32_noalloc_max_blocks", C.c_int64, []),
     ("utl_unpack_batch_u32", C.c_int, [VP, C.c_size_t, VP, VP, VP, C.c_int, C.c_int64, VP, VP, VP, VP]),
     ("utl_unpack_batch_u64", C.c_int, [VP, C.c_size_t, VP, VP, VP, C.c_int, C.c_int64, VP, VP, VP, VP]),
     ("utl_get_batch_u32", C.c_int, [VP, C.c_size_t, VP, VP, VP, C.c_int, VP, VP, C.c_int64, VP, VP, VP, VP]),

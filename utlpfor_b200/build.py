@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libutlpfor_b200.so")
-SOURCES = ["utl_kernels.cu", "utl_capi.cu"]
+SOURCES = ["utl_kernels.cu", "utl_capi.cu", "utl_noalloc.cu"]
 HEADERS = ["utl_device.cuh", "utl_launch.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
