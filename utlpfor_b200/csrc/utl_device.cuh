@@ -126,13 +126,12 @@ __device__ __forceinline__ void choose_best_packed(uint64_t c, int* best_w, int*
   for (int si = 0; si < 8; si++) max_si += ((c >> (8 * si)) & 0xFF) != 0;
   int bw = max_si * 4, be = 0;
   int best = 4 + (max_si << 6);
-  // excCostBytesPerValue, select_bitwidth.go:35: nibble d-1 holds the entry of step delta d
-  const uint32_t bpv_lut = 0x44332211u;
 #pragma unroll
   for (int si = 7; si >= 0; si--) {
     const int e = (int)((c >> (8 * si)) & 0xFF);
-    const int delta = max_si - si;
-    const int bpv = (int)((bpv_lut >> ((4 * (delta - 1)) & 31)) & 0xF);
+    // excCostBytesPerValue (select_bitwidth.go:35) is {1,1,1,2,2,3,3,4,4}:
+    // for the step deltas 1..8 that occur, (delta + 1) / 2
+    const int bpv = (max_si - si + 1) >> 1;
     const int cost = 4 + (si << 6) + 2 + min(e, 16) + ((e + 3) >> 2) + e * bpv;
     if (si < max_si && cost < best) {
       best = cost;

@@ -251,8 +251,8 @@ __device__ __forceinline__ void tile_resolve_issue(const uint64_t* status, int64
 }
 // Finish the look-back started by tile_resolve_issue (whole warp) and
 // publish the tile's inclusive prefix.
-__device__ uint64_t tile_resolve_finish(uint64_t* status, int64_t tile, uint64_t agg, int lane, uint32_t* err,
-                                        LookRound& r) {
+__device__ __forceinline__ uint64_t tile_resolve_finish(uint64_t* status, int64_t tile, uint64_t agg, int lane,
+                                                       uint32_t* err, LookRound& r) {
   if (tile == 0) return 0;
   uint64_t excl = 0;
   int64_t j = tile - 1;
@@ -297,6 +297,15 @@ __device__ uint64_t tile_resolve_finish(uint64_t* status, int64_t tile, uint64_t
   if (__any_sync(kFull, timed_out) && lane == 0 && err) atomicOr(err, 1u << 10);
   if (lane == 0) st_relaxed_u64(&status[tile], ((excl + agg) << 2) | 2u);
   return excl;
+}
+
+// Look-back of a tile whose aggregate is already published, in one go (out
+// of line: used only for tiles too large for the pack's image).
+__device__ __noinline__ uint64_t tile_resolve_now(uint64_t* status, int64_t tile, uint64_t agg, int lane,
+                                                  uint32_t* err) {
+  LookRound r;
+  tile_resolve_issue(status, tile, lane, r);
+  return tile_resolve_finish(status, tile, agg, lane, err, r);
 }
 
 __device__ uint64_t tile_lookback(uint64_t* status, int64_t tile, uint64_t agg, int lane, uint32_t* err) {
@@ -557,12 +566,14 @@ __global__ void __launch_bounds__(kQThreads) unpack_quad_kernel(UnpackArgs a) {
 
 struct QuadPackSmem {
   uint32_t hb[kQTile][kBlock];
+  uint32_t xs[kQTile][kBlock];
   uint8_t idx[kQTile][16];
   uint4 image[2][kQImage / 16 + 2];
   int len[2][kQTile];
   int off[2][kQTile + 1];
   int64_t tile[2];
   uint64_t prefix;
+  uint64_t direct_prefix;
   int64_t next;
 };
 
@@ -640,14 +651,13 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
           const uint4 t = __ldcs((const uint4*)(vp + 16 * v + 4 * j));
           x[v][0] = t.x; x[v][1] = t.y; x[v][2] = t.z; x[v][3] = t.w;
         }
-        plan = quad::quad_plan_block<true>(x, n, a.flag, kTypeU32, kModePlain, S.hb[lb], S.idx[lb], j, qm);
       } else {
 #pragma unroll
         for (int v = 0; v < 8; v++)
 #pragma unroll
           for (int k = 0; k < 4; k++) x[v][k] = (16 * v + 4 * j + k < n) ? __ldcs(vp + 16 * v + 4 * j + k) : 0u;
-        plan = quad::quad_plan_block<false>(x, n, a.flag, kTypeU32, kModePlain, S.hb[lb], S.idx[lb], j, qm);
       }
+      plan = quad::quad_plan_block(x, n, a.flag, kTypeU32, kModePlain, S.hb[lb], S.idx[lb], S.xs[lb], j, qm);
     }
     if (j == 0) S.len[cb][lb] = plan.len;
     __syncthreads();
@@ -673,6 +683,18 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
     }
     __syncthreads();
 
+    // a tile too large for the image is resolved now and written straight
+    // to HBM in phase C
+    const int total = tile >= 0 ? S.off[cb][kQTile] : 0;
+    const bool direct = total > kQImage;
+    if (direct) {
+      if (warp == 0) {
+        const uint64_t pre = tile_resolve_now(a.tile_status, tile, (uint64_t)total, lane, a.err);
+        if (lane == 0) S.direct_prefix = pre;
+      }
+      __syncthreads();
+    }
+
     // phase D of t_{i-1}
     if (ptile >= 0) {
       const uint64_t G = S.prefix;
@@ -688,35 +710,24 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
       else if (tid == 0 && a.err) atomicOr(a.err, 1u << 9);
     }
 
-    // phase C of t_i
+    // phase C of t_i: into the image, or straight to HBM
     if (tile >= 0) {
-      const int total = S.off[cb][kQTile];
-      if (total <= kQImage) {
-        if (live)
-          quad::quad_write_block(plan, x, kModePlain, 0, S.hb[lb], S.idx[lb], (uint8_t*)S.image[cb] + S.off[cb][lb],
-                                 j, qm);
-      } else {
-        // too large for the image: resolve now and write straight to HBM
-        __syncthreads();
-        if (warp == 0) {
-          LookRound r2;
-          tile_resolve_issue(a.tile_status, tile, lane, r2);
-          const uint64_t pre = tile_resolve_finish(a.tile_status, tile, (uint64_t)total, lane, a.err, r2);
-          if (lane == 0) S.prefix = pre;
-        }
-        __syncthreads();
-        const uint64_t G = S.prefix;
+      uint8_t* o = (uint8_t*)S.image[cb] + S.off[cb][lb];
+      bool write = live;
+      if (direct) {
+        const uint64_t G = S.direct_prefix;
         const bool fits = G + (uint64_t)total <= a.out_cap;
         if (live && j == 0) {
           const uint64_t g = G + (uint64_t)S.off[cb][lb];
           a.block_off[b] = g;
           if (b == a.n_blocks - 1) a.block_off[a.n_blocks] = g + (uint64_t)plan.len;
         }
-        if (fits && live)
-          quad::quad_write_block(plan, x, kModePlain, 0, S.hb[lb], S.idx[lb], a.out + G + S.off[cb][lb], j, qm);
         if (!fits && tid == 0 && a.err) atomicOr(a.err, 1u << 9);
-        if (tid == 0) S.tile[cb] = -1;  // nothing pending
+        write = live && fits;
+        o = a.out + G + S.off[cb][lb];
       }
+      if (write) quad::quad_write_block(plan, x, kModePlain, 0, S.hb[lb], S.idx[lb], o, j, qm);
+      if (direct && tid == 0) S.tile[cb] = -1;  // nothing pending
     }
   }
 }

@@ -83,6 +83,45 @@ __device__ __forceinline__ void load16<SmemBytes>(const SmemBytes& s, int64_t a,
   w[3] = __funnelshift_r(w3, w4, sh);
 }
 
+// Bitmap-mode high bits (more than 16 exceptions): lane j sizes control
+// bytes 8j..8j+7 (exceptions.go:63-80 validation), then decodes its values
+// into patch[rank], pre-shifted by bw.  Returns false on a corrupt region.
+template <class Src>
+__device__ __forceinline__ bool decode_bitmap_high_bits(const Src& sb, int64_t svb, int exc, int nc, int svb_len,
+                                                     int bw, uint32_t* patch, int j, unsigned qm) {
+  int tot = 0;
+  for (int g8 = 0; g8 < 8; g8++) {
+    const int g = 8 * j + g8;
+    if (g < nc) {
+      const uint32_t c = sb.u8(svb + g);
+      const int sl = min(4, exc - 4 * g);
+      const uint32_t m = sl >= 4 ? 0xFFu : ((1u << (2 * sl)) - 1u);
+      tot += sl + sum2bit(c & m);
+    }
+  }
+  const int before = (int)qexcl((uint32_t)tot, j, qm);
+  const int needed = nc + (int)qsum((uint32_t)tot, qm);
+  if (needed > svb_len) return false;
+  __syncwarp(qm);
+  int64_t d = svb + nc + before;
+  for (int g8 = 0; g8 < 8; g8++) {
+    const int g = 8 * j + g8;
+    if (g < nc) {
+      const uint32_t c = sb.u8(svb + g);
+      const int sl = min(4, exc - 4 * g);
+      for (int s2 = 0; s2 < sl; s2++) {
+        const int l = (int)((c >> (2 * s2)) & 3) + 1;
+        uint32_t hv = sb.u32(d);
+        if (l < 4) hv &= (1u << (8 * l)) - 1u;
+        patch[4 * g + s2] = shl32(hv, bw);
+        d += l;
+      }
+    }
+  }
+  __syncwarp(qm);
+  return true;
+}
+
 // Unpack one uint32 block (unpackUint32Scalar, scalar.go:260-309, with
 // decodeUnpackHeader unpack_block.go:62-172 and applyExceptions
 // exceptions.go:194-284).  x[v][c] receives position 16v+4j+c.  patch is
@@ -201,46 +240,12 @@ __device__ QResult quad_unpack_block(const Src& sb, int64_t blk, int64_t avail, 
         x[v][0] = t.x; x[v][1] = t.y; x[v][2] = t.z; x[v][3] = t.w;
       }
     } else {
-      // Bitmap mode: decode every high-bit value into patch[] (thread j
-      // takes control bytes 8j..8j+7), then each lane ORs the ranks of its
-      // own positions.
-      uint32_t gs[8];
-      int tot = 0;
-#pragma unroll
-      for (int g8 = 0; g8 < 8; g8++) {
-        const int g = 8 * j + g8;
-        int s = 0;
-        if (g < nc) {
-          const uint32_t c = sb.u8(svb + g);
-          const int sl = min(4, exc - 4 * g);
-          const uint32_t m = sl >= 4 ? 0xFFu : ((1u << (2 * sl)) - 1u);
-          s = sl + sum2bit(c & m);
-        }
-        gs[g8] = (uint32_t)s;
-        tot += s;
+      // Bitmap mode: decode every high-bit value into patch[] (out of
+      // line: rare), then each lane ORs the ranks of its own positions.
+      if (!decode_bitmap_high_bits(sb, svb, exc, nc, svb_len, bw, patch, j, qm)) {
+        r.status = kErrInvalidBuffer;
+        return r;
       }
-      const int before = (int)qexcl((uint32_t)tot, j, qm);
-      const int needed = nc + (int)qsum((uint32_t)tot, qm);
-      if (needed > svb_len) { r.status = kErrInvalidBuffer; return r; }
-      __syncwarp(qm);
-      int64_t d = svb + nc + before;
-#pragma unroll
-      for (int g8 = 0; g8 < 8; g8++) {
-        const int g = 8 * j + g8;
-        if (g < nc) {
-          const uint32_t c = sb.u8(svb + g);
-          const int sl = min(4, exc - 4 * g);
-          for (int s2 = 0; s2 < sl; s2++) {
-            const int l = (int)((c >> (2 * s2)) & 3) + 1;
-            uint32_t hv = sb.u32(d);
-            if (l < 4) hv &= (1u << (8 * l)) - 1u;
-            patch[4 * g + s2] = shl32(hv, bw);
-            d += l;
-          }
-        }
-        (void)gs[g8];
-      }
-      __syncwarp(qm);
       uint32_t rowbits[8];
       int pop = 0;
 #pragma unroll
@@ -336,16 +341,14 @@ __device__ __forceinline__ uint32_t shl_clamp(uint32_t x, uint32_t s) {
 // 1 << (clz & ~3) to a word of eight 4-bit counters; the values are split
 // over three words so no counter exceeds 15, then the nibbles are widened
 // to bytes: E holds buckets 0,2,4,6 and O buckets 1,3,5,7.
-template <bool kAll>
-__device__ __forceinline__ void bucket_hist(const uint32_t (&x)[8][4], int n, int j, uint32_t& E, uint32_t& O) {
+// Positions past the block's count hold zero and land in the dropped
+// bucket 8.
+__device__ __forceinline__ void bucket_hist(const uint32_t (&x)[8][4], uint32_t& E, uint32_t& O) {
   uint32_t acc[3] = {0, 0, 0};
 #pragma unroll
   for (int v = 0; v < 8; v++)
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const uint32_t add = shl_clamp(1u, (uint32_t)__clz(x[v][k]) & ~3u);
-      if (kAll || 16 * v + 4 * j + k < n) acc[(4 * v + k) / 11] += add;
-    }
+    for (int k = 0; k < 4; k++) acc[(4 * v + k) / 11] += shl_clamp(1u, (uint32_t)__clz(x[v][k]) & ~3u);
   E = (acc[0] & 0x0F0F0F0Fu) + (acc[1] & 0x0F0F0F0Fu) + (acc[2] & 0x0F0F0F0Fu);
   O = ((acc[0] >> 4) & 0x0F0F0F0Fu) + ((acc[1] >> 4) & 0x0F0F0F0Fu) + ((acc[2] >> 4) & 0x0F0F0F0Fu);
 }
@@ -368,21 +371,16 @@ __device__ __forceinline__ uint64_t quad_exc_from_buckets(uint32_t E, uint32_t O
 
 // Phase A: FOR (for.go:95-126), delta/zigzag (delta.go:23-48), width
 // (select_bitwidth.go:20-72), exception ranks and high bits (exceptions.go:
-// 138-186) and the StreamVByte length.  x[v][c] is turned into the work
-// values in place (positions >= n become 0).  hb (128 words, 16-byte
+// 138-186) and the StreamVByte length.  x[v][c] holds the block's values,
+// zero past position n (the reference packs zeros there, scalar.go:34-40),
+// and is turned into the work values in place.  hb (128 words, 16-byte
 // aligned) receives the high bits in rank order and idx (16 bytes) the
-// position list or bitmap.  kAll: the block is full (n == 128).
-template <bool kAll>
+// position list or bitmap.  mode as in warp_pack_block.  Partial blocks
+// (n < 128) take masked variants of the steps that must skip padding.
 __device__ QPlan quad_plan_block(uint32_t (&x)[8][4], int n, int flag, uint32_t type_flags, int mode,
-                                 uint32_t* hb, uint8_t* idx, int j, unsigned qm) {
-#define QVALID(v, k) (kAll || 16 * (v) + 4 * j + (k) < n)
-  if (!kAll) {
-#pragma unroll
-    for (int v = 0; v < 8; v++)
-#pragma unroll
-      for (int k = 0; k < 4; k++)
-        if (!QVALID(v, k)) x[v][k] = 0;
-  }
+                                 uint32_t* hb, uint8_t* idx, uint32_t* xs, int j, unsigned qm) {
+  const bool full = n == kBlock;
+#define QVALID(v, k) (16 * (v) + 4 * j + (k) < n)
   uint32_t hflags = type_flags | ((uint32_t)(flag & kSpecial) << 14);
   bool use_for = false;
   uint32_t base = 0;
@@ -391,20 +389,30 @@ __device__ QPlan quad_plan_block(uint32_t (&x)[8][4], int n, int flag, uint32_t 
   bool have_hist = false;
   if (!(flag & kNoFOR)) {
     uint32_t mn = 0xFFFFFFFFu, mx = 0u;
+    if (full) {
 #pragma unroll
-    for (int v = 0; v < 8; v++)
+      for (int v = 0; v < 8; v++)
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        if (QVALID(v, k)) mn = min(mn, x[v][k]);
-        mx = max(mx, x[v][k]);  // padding is zero
-      }
+        for (int k = 0; k < 4; k++) {
+          mn = min(mn, x[v][k]);
+          mx = max(mx, x[v][k]);
+        }
+    } else {
+#pragma unroll
+      for (int v = 0; v < 8; v++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          if (QVALID(v, k)) mn = min(mn, x[v][k]);
+          mx = max(mx, x[v][k]);  // padding is zero
+        }
+    }
     mn = qmin(mn, qm);
     mx = qmax(mx, qm);
     if (mn != 0) {
       const int for_max = round_step(len32(mx - mn));
       const int raw_max = round_step(len32(mx));
       if (for_max < raw_max) {
-        bucket_hist<kAll>(x, n, j, h_e, h_o);
+        bucket_hist(x, h_e, h_o);
         have_hist = true;
         int std_w, dummy;
         choose_best_packed(quad_exc_from_buckets(h_e, h_o, qm), &std_w, &dummy);
@@ -420,8 +428,7 @@ __device__ QPlan quad_plan_block(uint32_t (&x)[8][4], int n, int flag, uint32_t 
 #pragma unroll
       for (int v = 0; v < 8; v++)
 #pragma unroll
-        for (int k = 0; k < 4; k++)
-          if (QVALID(v, k)) x[v][k] -= base;
+        for (int k = 0; k < 4; k++) x[v][k] = (full || QVALID(v, k)) ? x[v][k] - base : 0u;
       hflags |= (uint32_t)fw << 15;
       have_hist = false;
     }
@@ -432,7 +439,7 @@ __device__ QPlan quad_plan_block(uint32_t (&x)[8][4], int n, int flag, uint32_t 
     for (int k = 0; k < 4; k++)
 #pragma unroll
       for (int v = 7; v >= 1; v--)
-        if (QVALID(v, k)) {
+        if (full || QVALID(v, k)) {
           borrow |= x[v][k] < x[v - 1][k];
           x[v][k] -= x[v - 1][k];
         }
@@ -441,8 +448,7 @@ __device__ QPlan quad_plan_block(uint32_t (&x)[8][4], int n, int flag, uint32_t 
 #pragma unroll
       for (int v = 0; v < 8; v++)
 #pragma unroll
-        for (int k = 0; k < 4; k++)
-          if (QVALID(v, k)) x[v][k] = zz_enc(x[v][k]);
+        for (int k = 0; k < 4; k++) x[v][k] = zz_enc(x[v][k]);  // zz_enc(0) == 0 keeps the padding
     }
     hflags |= kHdrDelta | (zz ? kHdrZigZag : 0u);
     have_hist = false;
@@ -456,7 +462,7 @@ __device__ QPlan quad_plan_block(uint32_t (&x)[8][4], int n, int flag, uint32_t 
       for (int k = 0; k < 4; k++) o |= x[v][k];
     bw = round_step(len32(qor(o, qm)));
   } else {
-    if (!have_hist) bucket_hist<kAll>(x, n, j, h_e, h_o);
+    if (!have_hist) bucket_hist(x, h_e, h_o);
     choose_best_packed(quad_exc_from_buckets(h_e, h_o, qm), &bw, &exc_n);
   }
   QPlan p;
@@ -494,20 +500,20 @@ __device__ QPlan quad_plan_block(uint32_t (&x)[8][4], int n, int flag, uint32_t 
     const uint32_t sl = (tl * 0x01010101u) >> 24;  // all rows 0-3
     const uint32_t bl = tl * 0x01010100u + el;      // byte v: rank base of row v
     const uint32_t bh = th * 0x01010100u + sl * 0x01010101u + eh;
+    // the work values go through shared memory so that only the set flag
+    // bits are visited (about 0.1 per lane for typical data)
     __syncwarp(qm);
 #pragma unroll
-    for (int v = 0; v < 8; v++) {
+    for (int v = 0; v < 8; v++) *(uint4*)(xs + 16 * v + 4 * j) = make_uint4(x[v][0], x[v][1], x[v][2], x[v][3]);
+    for (uint32_t m = nibs; m; m &= m - 1) {
+      const int i = __ffs(m) - 1;
+      const int v = i >> 2, k = i & 3;
       const uint32_t nib = (nibs >> (4 * v)) & 0xFu;
-      if (nib) {
-        const int rb = (int)(((v < 4 ? bl : bh) >> (8 * (v & 3))) & 0xFF);
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-          if ((nib >> k) & 1u) {
-            const int r = rb + __popc(nib & ((1u << k) - 1u));
-            hb[r] = x[v][k] >> bw;
-            if (exc_n <= 16) idx[r] = (uint8_t)(16 * v + 4 * j + k);
-          }
-      }
+      const int rb = (int)(((v < 4 ? bl : bh) >> (8 * (v & 3))) & 0xFF);
+      const int r = rb + __popc(nib & ((1u << k) - 1u));
+      const int pos = 16 * v + 4 * j + k;
+      hb[r] = xs[pos] >> bw;
+      if (exc_n <= 16) idx[r] = (uint8_t)pos;
     }
     if (exc_n > 16) {
       // bitmap: bytes 2v, 2v+1 hold row v's 16 lane flags, LSB first
