@@ -303,6 +303,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--log2n", type=int, default=28, help="values per GPU of the c3 workloads (2^log2n)")
+    ap.add_argument("--knob", action="append", default=[], help="kernel knob id=value (see utl_set_knob)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -326,11 +327,14 @@ def main():
     wl = WORKLOADS[args.workload]
     flag, is64 = wl["flag"], wl["is64"]
     esz = 8 if is64 else 4
+    L = load()
+    for kv in args.knob:
+        k, v = kv.split("=")
+        assert L.utl_set_knob(int(k), int(v)) == 0, kv
     values, vo = make_workload(torch, args.workload, rank, dev, args.log2n)
     n = int(vo[-1])
     codec = U.BatchCodec(vo, flag=flag, is64=is64, device=dev)
     out = torch.empty_like(values)
-    L = load()
 
     def barrier():
         if world > 1:

@@ -249,6 +249,19 @@ UTL_API int utl_unpack_streams_u64(const uint8_t *h_packed, size_t packed_len,
                            const uint64_t *h_val_off, int n_streams,
                            uint64_t *h_values);
 
+/* ==================== tuning ==================== */
+/* Process-wide knobs of the batched kernels, set by the autotuner
+ * (utlpfor_b200.tune); no counterpart in the reference.  Defaults are
+ * sound on any B200.
+ *   UTL_KNOB_UNPACK_SCHEDULE: 0 = one CTA per 32 blocks, 1 = persistent
+ *     warps with the next group's bytes in flight (cp.async double buffer).
+ *   UTL_KNOB_PACK_CTAS_PER_SM: cap on resident pack CTAs per SM (0 = the
+ *     occupancy maximum). */
+#define UTL_KNOB_UNPACK_SCHEDULE 0
+#define UTL_KNOB_PACK_CTAS_PER_SM 1
+UTL_API int utl_set_knob(int knob, int value);
+UTL_API int utl_get_knob(int knob);
+
 /* ==================== diagnostics ==================== */
 /* Number of this library's kernels launched so far in this process. */
 UTL_API uint64_t utl_launch_count(void);

@@ -27,9 +27,19 @@ def to_dev(torch, a):
 LENS = [1, 128, 300, 0, 257, 1000, 5, 129, 0, 4096, 77]
 
 
+@pytest.fixture(params=[0, 1], ids=["unpack_tiles", "unpack_pipelined"])
+def sched(request):
+    from utlpfor_b200._lib import load
+    L = load()
+    old = L.utl_get_knob(0)
+    assert L.utl_set_knob(0, request.param) == 0
+    yield request.param
+    L.utl_set_knob(0, old)
+
+
 @pytest.mark.parametrize("flag", range(8))
 @pytest.mark.parametrize("kind", ["small", "exc", "dense_exc", "sorted", "walk", "wide", "const"])
-def test_pack_unpack_batch_u32(env, flag, kind):
+def test_pack_unpack_batch_u32(env, flag, kind, sched):
     U, torch = env
     rng = np.random.default_rng(flag * 31 + len(kind))
     vals, vo = streams(rng, LENS, kind)
@@ -104,7 +114,7 @@ def test_get_batch(env, is64, flag):
                 assert out[i] == gv == vals[int(vo[s]) + p]
 
 
-def test_unpack_batch_corrupt_blocks(env):
+def test_unpack_batch_corrupt_blocks(env, sched):
     """A corrupt block fails its own status only; the others decode."""
     U, torch = env
     rng = np.random.default_rng(3)
@@ -144,7 +154,7 @@ def test_host_buffer_streams(env):
         assert np.array_equal(out, vals)
 
 
-def test_large_round_trip_properties(env):
+def test_large_round_trip_properties(env, sched):
     """2^24 values with the exception-heavy shape: pack is byte-identical to
     the oracle (checked by digest), unpack restores every value."""
     U, torch = env

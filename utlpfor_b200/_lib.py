@@ -55,6 +55,8 @@ SIGNATURES = [
     ("utl_pack_streams_u64", C.c_int, [C.c_uint8, VP, PU64, C.c_int, VP, C.c_size_t, PU64, PU64, SZ]),
     ("utl_unpack_streams_u32", C.c_int, [VP, C.c_size_t, PU64, PU64, C.c_int, VP]),
     ("utl_unpack_streams_u64", C.c_int, [VP, C.c_size_t, PU64, PU64, C.c_int, VP]),
+    ("utl_set_knob", C.c_int, [C.c_int, C.c_int]),
+    ("utl_get_knob", C.c_int, [C.c_int]),
     ("utl_launch_count", C.c_uint64, []),
     ("utl_last_cuda_error", C.c_int, []),
     ("utl_version", C.c_char_p, []),

@@ -198,9 +198,12 @@ class BatchCodec:
     values/out are CUDA tensors of the element size (4 or 8 bytes).
     """
 
-    def __init__(self, val_off_host, flag=0, is64=False, device="cuda", out_cap=None):
+    def __init__(self, val_off_host, flag=0, is64=False, device="cuda", out_cap=None, tuned=True):
         torch = _torch()
         L = load()
+        if tuned:
+            from .tune import apply
+            apply(device)
         vo = np.ascontiguousarray(val_off_host, dtype=np.uint64)
         self.n_streams = len(vo) - 1
         self.n_blocks = count_blocks(vo)
@@ -237,6 +240,20 @@ class BatchCodec:
         _check(self._get_fn(_ptr(self.packed), self.packed.numel(), _ptr(self.block_off), _ptr(self.val_off),
                             _ptr(self.block_start), self.n_streams, _ptr(q_stream), _ptr(q_pos), q_stream.numel(),
                             _ptr(out), _ptr(status), _ptr(self.err), _stream()))
+
+    def capture(self, values, out):
+        """Record pack(values) + unpack(out) into a CUDA graph (one warm-up
+        pass runs first so no first-use setup happens during capture);
+        returns the torch.cuda.CUDAGraph to replay()."""
+        torch = _torch()
+        self.pack(values)
+        self.unpack(out)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.pack(values)
+            self.unpack(out)
+        return g
 
     @property
     def packed_len(self):

@@ -652,6 +652,9 @@ int utl_unpack_streams_u64(const uint8_t* h_packed, size_t packed_len, const uin
   return unpack_streams(true, h_packed, packed_len, h_block_off, h_val_off, n_streams, h_values);
 }
 
+int utl_set_knob(int knob, int value) { return launch::set_knob(knob, value) == 0 ? UTL_OK : UTL_ERR_ARG; }
+int utl_get_knob(int knob) { return launch::get_knob(knob); }
+
 uint64_t utl_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 int utl_last_cuda_error(void) { return t_last_cuda; }
 const char* utl_version(void) { return "utlpfor-b200 0.1 (sm_100a)"; }

@@ -564,6 +564,165 @@ __global__ void __launch_bounds__(kQThreads) unpack_quad_kernel(UnpackArgs a) {
   }
 }
 
+// Pipelined variant: persistent warps walk groups of 8 blocks with a stride
+// of the whole grid; while a warp decodes group g its next group's bytes
+// are already in flight into the second staging buffer (cp.async, 16-byte
+// chunks, no registers held) and the block offsets of the group after
+// that are loading.  Groups that do not fit a buffer take the one-block-
+// per-round path of unpack_quad_kernel.
+constexpr int kPStage = 8 * 264;  // per-buffer budget: 8 blocks of up to 264 bytes
+struct QuadPipeSmem {
+  uint4 stage[kQWarps][2][(kPStage + kQStagePad) / 16];
+  uint4 patch[kQWarps][8][kBlock / 4];
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Issue the staging of bytes [g0, g1) of buf as stage_bytes lays them out;
+// chunks that are not wholly inside the buffer are copied synchronously.
+__device__ __forceinline__ void stage_bytes_async(uint4* dst16, const uint8_t* buf, uint64_t buf_len, uint64_t g0,
+                                                  uint64_t g1, int lane) {
+  const uintptr_t lo = (uintptr_t)buf, hi = lo + buf_len;
+  const uintptr_t a0 = (lo + g0) & ~(uintptr_t)15;
+  const uintptr_t a1 = (lo + g1 + 15) & ~(uintptr_t)15;
+  const int nch = (int)((a1 - a0) >> 4);
+  for (int c = lane; c < nch; c += 32) {
+    const uintptr_t a = a0 + 16 * (uintptr_t)c;
+    if (a >= lo && a + 16 <= hi) {
+      cp_async16(&dst16[c], (const void*)a);
+    } else {
+      uint32_t w[4] = {0, 0, 0, 0};
+      for (int bb = 0; bb < 16; bb++) {
+        const uintptr_t x = a + bb;
+        if (x >= lo && x < hi) w[bb >> 2] |= (uint32_t)(*(const uint8_t*)x) << ((bb & 3) * 8);
+      }
+      dst16[c] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+}
+
+struct GroupInfo {
+  uint64_t off;   // lane l <= nb: block_off[b0 + l]
+  int64_t b0;
+  int nb;
+};
+
+__device__ __forceinline__ GroupInfo group_load(const UnpackArgs& a, int64_t g, int lane) {
+  GroupInfo gi;
+  gi.b0 = g * 8;
+  gi.nb = gi.b0 < a.n_blocks ? (int)min((int64_t)8, a.n_blocks - gi.b0) : 0;
+  gi.off = (gi.nb > 0 && lane <= gi.nb) ? a.block_off[gi.b0 + lane] : 0ull;
+  return gi;
+}
+
+// whether a group's contiguous bytes fit one staging buffer (warp-uniform)
+__device__ __forceinline__ bool group_fits(const UnpackArgs& a, const GroupInfo& gi, int lane) {
+  const uint64_t next = __shfl_down_sync(kFull, gi.off, 1);
+  const bool ok = lane >= gi.nb || (next >= gi.off && next - gi.off <= (uint64_t)kMaxBlock32 && next <= a.packed_len);
+  const uint64_t o0 = __shfl_sync(kFull, gi.off, 0), o1 = __shfl_sync(kFull, gi.off, gi.nb);
+  const int ph = (int)(((uintptr_t)a.packed + o0) & 15);
+  return __all_sync(kFull, ok) && (int64_t)(o1 - o0) + ph + 16 <= kPStage;
+}
+
+__global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackArgs a) {
+  extern __shared__ uint4 smem4[];
+  QuadPipeSmem& S = *(QuadPipeSmem*)smem4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int q = lane >> 2, j = lane & 3;
+  const unsigned qm = quad::quad_mask(lane);
+  const int64_t n_groups = (a.n_blocks + 7) / 8;
+  const int64_t stride = (int64_t)gridDim.x * kQWarps;
+  int64_t g = (int64_t)blockIdx.x * kQWarps + warp;
+  if (g >= n_groups) return;
+  uint32_t* patch = (uint32_t*)S.patch[warp][q];
+
+  GroupInfo cur = group_load(a, g, lane);
+  bool cur_fits = group_fits(a, cur, lane);
+  if (cur_fits)
+    stage_bytes_async(S.stage[warp][0], a.packed, a.packed_len, __shfl_sync(kFull, cur.off, 0),
+                      __shfl_sync(kFull, cur.off, cur.nb), lane);
+  cp_async_commit();
+  GroupInfo nxt = group_load(a, g + stride, lane);
+  for (int it = 0; g < n_groups; it++, g += stride) {
+    const int buf = it & 1;
+    // put the next group in flight, and start loading the one after it
+    const bool nxt_fits = nxt.nb > 0 && group_fits(a, nxt, lane);
+    if (nxt_fits)
+      stage_bytes_async(S.stage[warp][buf ^ 1], a.packed, a.packed_len, __shfl_sync(kFull, nxt.off, 0),
+                        __shfl_sync(kFull, nxt.off, nxt.nb), lane);
+    cp_async_commit();
+    const GroupInfo nn = group_load(a, g + 2 * stride, lane);
+    cp_async_wait1();
+    __syncwarp();
+
+    const int nb = cur.nb;
+    const uint64_t off0 = __shfl_sync(kFull, cur.off, 0);
+    const uint64_t s = __shfl_sync(kFull, cur.off, q), e = __shfl_sync(kFull, cur.off, q + 1);
+    const bool bad = e < s || e - s > (uint64_t)kMaxBlock32 || e > a.packed_len;
+    const int64_t b = cur.b0 + q;
+    const int rounds = cur_fits ? 1 : nb;
+    const uint4* stg = S.stage[warp][buf];
+#pragma unroll 1
+    for (int rd = 0; rd < rounds; rd++) {
+      if (!cur_fits) {
+        // one block per round, synchronously, through this group's buffer
+        const uint64_t rs = __shfl_sync(kFull, cur.off, rd), re = __shfl_sync(kFull, cur.off, rd + 1);
+        __syncwarp();
+        if (re >= rs && re - rs <= (uint64_t)kMaxBlock32 && re <= a.packed_len)
+          stage_bytes(S.stage[warp][buf], a.packed, a.packed_len, rs, re, lane, 32);
+        __syncwarp();
+      }
+      if (cur_fits ? q < nb : q == rd) {
+        uint64_t first;
+        int want;
+        block_span(a.val_off, a.block_start, a.n_streams, b, &first, &want);
+        int status = kOK, ovf = 0;
+        if (bad) {
+          status = kErrCountMismatch;
+        } else {
+          const int len = (int)(e - s);
+          const int blk = cur_fits ? (int)(((uintptr_t)a.packed + off0) & 15) + (int)(s - off0)
+                                   : (int)(((uintptr_t)a.packed + s) & 15);
+          uint32_t x[8][4];
+          const quad::QResult r =
+              quad::quad_unpack_block(SmemBytes{(const uint32_t*)stg}, blk, len, false, x, patch, j, qm);
+          status = r.status;
+          ovf = r.ovf;
+          if (status == kOK && (r.count != want || r.consumed != len)) status = kErrCountMismatch;
+          if (status == kOK) {
+            uint32_t* op = (uint32_t*)a.values + first;
+            if (want == kBlock && ((uintptr_t)op & 15) == 0) {
+#pragma unroll
+              for (int v = 0; v < 8; v++)
+                __stcs((uint4*)(op + 16 * v + 4 * j), make_uint4(x[v][0], x[v][1], x[v][2], x[v][3]));
+            } else {
+#pragma unroll
+              for (int v = 0; v < 8; v++)
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                  if (16 * v + 4 * j + k < want) op[16 * v + 4 * j + k] = x[v][k];
+            }
+          }
+        }
+        if (j == 0) {
+          if (a.block_status) a.block_status[b] = status | (ovf << 8);
+          if (status != kOK && a.err) atomicOr(a.err, 1u << status);
+        }
+      }
+    }
+    __syncwarp();
+    cur = nxt;
+    cur_fits = nxt_fits;
+    nxt = nn;
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 struct QuadPackSmem {
   uint32_t hb[kQTile][kBlock];
   uint32_t xs[kQTile][kBlock];
@@ -623,10 +782,12 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
   const unsigned qm = quad::quad_mask(lane);
   const int lb = warp * 8 + q;  // block within the tile
 
-  if (tid == 0) S.tile[1] = -1;  // no pending tile
+  if (tid == 0) {
+    S.tile[1] = -1;  // no pending tile
+    S.next = (int64_t)atomicAdd((unsigned long long*)a.counter, 1ull);
+  }
   for (int it = 0;; it++) {
     const int cb = it & 1, pb = cb ^ 1;  // buffers of this and the pending tile
-    if (tid == 0) S.next = (int64_t)atomicAdd((unsigned long long*)a.counter, 1ull);
     __syncthreads();
     const int64_t tile = S.next < a.n_tiles ? S.next : -1;
     const int64_t ptile = S.tile[pb];
@@ -695,6 +856,11 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
       __syncthreads();
     }
 
+    // the next tile is taken now (its phase A follows phase C); the atomic's
+    // result is only stored at the end of the iteration
+    unsigned long long next_tile = 0;
+    if (tid == 0) next_tile = atomicAdd((unsigned long long*)a.counter, 1ull);
+
     // phase D of t_{i-1}
     if (ptile >= 0) {
       const uint64_t G = S.prefix;
@@ -729,6 +895,7 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
       if (write) quad::quad_write_block(plan, x, kModePlain, 0, S.hb[lb], S.idx[lb], o, j, qm);
       if (direct && tid == 0) S.tile[cb] = -1;  // nothing pending
     }
+    if (tid == 0) S.next = (int64_t)next_tile;
   }
 }
 
@@ -1058,6 +1225,10 @@ cudaError_t stream_offsets(const uint64_t* block_off, const uint64_t* bstart, in
 
 static int g_quad_pack_ctas = 0;
 static bool g_quad_unpack_cfg = false;
+static int g_pipe_ctas = 0;
+// 0: one CTA per 32 blocks; 1: persistent pipelined warps (selectable for tuning)
+static int g_unpack_schedule = 1;
+static int g_pack_cap = 0;
 
 cudaError_t pack(bool u64, const PackArgs& a_in, cudaStream_t st) {
   if (!u64) {
@@ -1071,7 +1242,8 @@ cudaError_t pack(bool u64, const PackArgs& a_in, cudaStream_t st) {
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_quad_pack_ctas, pack_quad_kernel, kQThreads, smem);
       if (g_quad_pack_ctas <= 0) g_quad_pack_ctas = 1;
     }
-    int64_t grid = (int64_t)num_sms() * g_quad_pack_ctas;
+    const int per_sm = (g_pack_cap > 0 && g_pack_cap < g_quad_pack_ctas) ? g_pack_cap : g_quad_pack_ctas;
+    int64_t grid = (int64_t)num_sms() * per_sm;
     if (grid > a.n_tiles) grid = a.n_tiles;
     if (grid < 1) grid = 1;
     pack_quad_kernel<<<(unsigned)grid, kQThreads, smem, st>>>(a);
@@ -1112,8 +1284,26 @@ cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
       cudaFuncSetAttribute(unpack_quad_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
       g_quad_unpack_cfg = true;
     }
+    if (a.n_blocks <= 0) return cudaSuccess;
+    if (g_unpack_schedule == 1) {
+      const size_t psmem = sizeof(QuadPipeSmem);
+      if (g_pipe_ctas == 0) {
+        cudaError_t e = cudaFuncSetAttribute(unpack_quad_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)psmem);
+        if (e != cudaSuccess) return e;
+        cudaFuncSetAttribute(unpack_quad_pipe_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_pipe_ctas, unpack_quad_pipe_kernel, kQThreads, psmem);
+        if (g_pipe_ctas <= 0) g_pipe_ctas = 1;
+      }
+      const int64_t groups = (a.n_blocks + 7) / 8;
+      int64_t grid = (int64_t)num_sms() * g_pipe_ctas;
+      const int64_t need = (groups + kQWarps - 1) / kQWarps;
+      if (grid > need) grid = need;
+      unpack_quad_pipe_kernel<<<(unsigned)grid, kQThreads, psmem, st>>>(a);
+      note_launch(1);
+      return cudaGetLastError();
+    }
     const int64_t grid = (a.n_blocks + kQTile - 1) / kQTile;
-    if (grid <= 0) return cudaSuccess;
     unpack_quad_kernel<<<(unsigned)grid, kQThreads, smem, st>>>(a);
     note_launch(1);
     return cudaGetLastError();
@@ -1165,6 +1355,27 @@ cudaError_t plain_get(bool u64, int pos, const uint8_t* src, int64_t staged, int
   else plain_get_kernel<false><<<1, 32, 0, st>>>(pos, src, staged, avail, tmp, res);
   note_launch(1);
   return cudaGetLastError();
+}
+
+int set_knob(int knob, int value) {
+  switch (knob) {
+    case 0:  // UTL_KNOB_UNPACK_SCHEDULE
+      if (value != 0 && value != 1) return -1;
+      g_unpack_schedule = value;
+      return 0;
+    case 1:  // UTL_KNOB_PACK_CTAS_PER_SM (0 = occupancy maximum)
+      if (value < 0 || value > 32) return -1;
+      g_pack_cap = value;
+      return 0;
+  }
+  return -1;
+}
+int get_knob(int knob) {
+  switch (knob) {
+    case 0: return g_unpack_schedule;
+    case 1: return g_pack_cap;
+  }
+  return -1;
 }
 
 }  // namespace launch

@@ -77,5 +77,7 @@ cudaError_t plain_unpack(bool u64, const uint8_t* src, int64_t staged, int64_t a
                          PlainResult* res, cudaStream_t st);
 cudaError_t plain_get(bool u64, int pos, const uint8_t* src, int64_t staged, int64_t avail, uint8_t* tmp,
                       PlainResult* res, cudaStream_t st);
+int set_knob(int knob, int value);
+int get_knob(int knob);
 }  // namespace launch
 }  // namespace utl
