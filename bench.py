@@ -17,7 +17,12 @@ C-ABI calls (utl_pack_streams_u32 / utl_unpack_streams_u32) with pinned
 host memory, copies included.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload c3|c3-nofor|c3-nopatch|c1|c2|c4]
+                    [--workload c3|c3-nofor|c3-nopatch|c1|c2|c4|c5]
+
+The c5 workload measures the serving loop instead (utlpfor_b200.serve):
+requests with host buffers arrive open-loop at swept Poisson rates; the
+line reports per-rate p50/p99 latency and sustained uncompressed GB/s, and
+the same request mix through the plain per-call C-ABI on a sample.
 """
 import argparse
 import ctypes as C
@@ -51,6 +56,9 @@ WORKLOADS = {
                flag=DELTA, is64=False),
     "c4": dict(desc="uint64_streams: 2^26 u64 in 512 streams, 1/3 FOR-reducible, 1/3 full-range, "
                     "1/3 random walks from 2^62 (flag Delta)", flag=DELTA, is64=True),
+    "c5": dict(desc="served_mixed_requests: Poisson arrivals, 60/30/10 decompress/compress/Get, sizes "
+                    "log-uniform [128,2^22] u32 drawn from the c1/c2/c3 distributions, 64 GB admission budget",
+               flag=0, is64=False),
 }
 
 
@@ -293,6 +301,181 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------
+# serving workload (c5)
+# --------------------------------------------------------------------------
+def c5_pools(seed, n=1 << 23):
+    """Host value pools of the c1/c2/c3 distributions; a request's values
+    are a contiguous slice of one pool."""
+    rng = np.random.default_rng(seed)
+    c1 = rng.integers(0, 2**11, n, dtype=np.uint64).astype(np.uint32)
+    c2 = np.cumsum(1 + rng.geometric(1 / 64, n)).astype(np.uint32)
+    c3 = c3_sample_host(n, seed + 1)
+    return [(c1, 0), (c2, DELTA), (c3, 0)]
+
+
+def c5_requests(rng, count, pools, n_resident):
+    """(kind, pool, start, size, handle index) per request: 60% decompress,
+    30% compress, 10% Get; sizes log-uniform in [128, 2^22]; a Get asks for
+    min(size/128, 4096) uniform positions of a resident stream."""
+    kinds = rng.choice(3, count, p=[0.6, 0.3, 0.1])
+    sizes = np.exp(rng.uniform(np.log(128), np.log(2**22), count)).astype(np.int64)
+    out = []
+    for k, sz in zip(kinds, sizes):
+        pi = int(rng.integers(0, len(pools)))
+        start = int(rng.integers(0, pools[pi][0].size - sz))
+        out.append((("decompress", "compress", "get")[k], pi, start, int(sz), int(rng.integers(0, n_resident))))
+    return out
+
+
+def run_serving(args):
+    import torch
+
+    import utlpfor_b200.serve as S
+    from utlpfor_b200._lib import load
+    L = load()
+    torch.cuda.set_device(0)
+    pools = c5_pools(5)
+    rng = np.random.default_rng(6)
+    budget = 64 << 30
+    srv = S.CodecServer(budget_bytes=budget, slots=args.serve_slots)
+    # resident streams the decompress/Get requests read
+    n_res = 64
+    res_specs = c5_requests(rng, n_res, pools, 1)
+    handles = [srv.submit_compress(pools[pi][0][st:st + sz], pools[pi][1]) for _, pi, st, sz, _ in res_specs]
+    handles = [f.result(timeout=300) for f in handles]
+    for h, (_, pi, st, sz, _) in zip(handles, res_specs):  # resident streams decode to their values
+        assert np.array_equal(srv.submit_decompress(h).result(timeout=300), pools[pi][0][st:st + sz])
+    errors = []
+
+    def submit(spec):
+        kind, pi, st, sz, hi = spec
+        if kind == "compress":
+            f = srv.submit_compress(pools[pi][0][st:st + sz], pools[pi][1])
+
+            def drop(fut):
+                if fut.exception() is not None:
+                    errors.append(repr(fut.exception()))
+                else:
+                    srv.release(fut.result())
+            f.add_done_callback(drop)
+            return
+        if kind == "decompress":
+            f = srv.submit_decompress(handles[hi])
+        else:
+            h = handles[hi]
+            q = min(max(sz // 128, 1), 4096)
+            f = srv.submit_get(h, (np.arange(q, dtype=np.int64) * 7919) % h.n_values)
+        f.add_done_callback(lambda fut: fut.exception() is not None and errors.append(repr(fut.exception())))
+
+    def run_point(specs, rate):
+        """Open-loop arrivals at `rate` requests/s (None: all at once)."""
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        gaps = rng.exponential(1.0 / rate, len(specs)) if rate else np.zeros(len(specs))
+        due = t0 + np.cumsum(gaps)
+        for spec, d in zip(specs, due):
+            w = d - time.perf_counter()
+            if w > 0:
+                time.sleep(w)
+            submit(spec)
+        srv.drain()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        return {"offered_req_per_s": rate, "requests": len(specs), "wall_s": round(wall, 3),
+                "served_req_per_s": round(len(specs) / wall, 1),
+                "sustained_GBps": round(st["uncompressed_bytes"] / wall / 1e9, 3),
+                "p50_ms": round(st["all"]["p50_ms"], 3), "p99_ms": round(st["all"]["p99_ms"], 3),
+                "by_kind": {k: {"p50_ms": round(st[k]["p50_ms"], 3), "p99_ms": round(st[k]["p99_ms"], 3)}
+                            for k in ("compress", "decompress", "get") if k in st},
+                "batches": st["batches"], "max_batches_in_flight": st["max_batches_in_flight"],
+                "admitted": st["admitted"], "rejected": st["rejected"]}
+
+    run_point(c5_requests(rng, 200, pools, n_res), None)   # warm-up: allocator caches, first launches
+    nreq = args.serve_requests
+    burst = run_point(c5_requests(rng, nreq, pools, n_res), None)
+    cap = burst["served_req_per_s"]
+    points = [run_point(c5_requests(rng, nreq, pools, n_res), round(cap * f, 1)) for f in (0.25, 0.5, 0.9)]
+    srv.close()
+
+    # the same mix through the plain per-call C-ABI (one call per block / position), on a sample
+    sample = c5_requests(np.random.default_rng(7), 40, pools, n_res)
+    res_bytes = []
+    for _, pi, st, sz, _ in res_specs:
+        pk, bo, _ = U_pack_host(pools[pi][0][st:st + sz], pools[pi][1])
+        res_bytes.append((pk, bo, sz))
+    t0 = time.perf_counter()
+    moved = 0
+    for kind, pi, st, sz, hi in sample:
+        if kind == "compress":
+            U_pack_host(pools[pi][0][st:st + sz], pools[pi][1], plain=L)
+            moved += 4 * sz
+        elif kind == "decompress":
+            pk, bo, n = res_bytes[hi]
+            U_unpack_host(pk, bo, n, L)
+            moved += 4 * n
+        else:
+            pk, bo, n = res_bytes[hi]
+            q = min(max(sz // 128, 1), 4096)
+            U_get_host(pk, bo, (np.arange(q, dtype=np.int64) * 7919) % n, L)
+            moved += 4 * q
+    plain_wall = time.perf_counter() - t0
+    best = max([burst] + points, key=lambda p: p["sustained_GBps"])
+    line = {"metric": "served sustained uncompressed GB/s (p50/p99 latency per offered rate)",
+            "value": best["sustained_GBps"], "unit": "GB/s", "n_gpus": 1, "steps": len(points) + 1,
+            "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded pools of the c1/c2/c3 distributions)",
+            "config": {"workload": WORKLOADS["c5"]["desc"], "requests_per_point": nreq,
+                       "resident_streams": n_res, "slots": args.serve_slots, "budget_bytes": budget,
+                       "results": "to host (numpy), inputs from host"},
+            "serving": {"burst": burst, "rates": points},
+            "plain_per_call": {"requests": len(sample), "GBps": round(moved / plain_wall / 1e9, 4),
+                               "wall_s": round(plain_wall, 2),
+                               "calls": "utl_pack_u32 / utl_unpack_u32 per 128-value block, utl_get_u32 per position"},
+            "errors": errors[:5], "gpu_launches": None}
+    print(json.dumps(line))
+    return 0
+
+
+def U_pack_host(values, flag, plain=None):
+    """Pack one stream block by block through the per-call C-ABI (plain) or
+    the batched host-buffer call; returns (packed, block_off, stream_off)."""
+    from utlpfor_b200 import batch
+    if plain is None:
+        return batch.pack_streams(flag, values, np.array([0, values.size], dtype=np.uint64))
+    buf = np.empty(600, dtype=np.uint8)
+    n = C.c_size_t(0)
+    pu8 = buf.ctypes.data_as(C.POINTER(C.c_uint8))
+    for i in range(0, values.size, 128):
+        blk = values[i:i + 128]
+        rc = plain.utl_pack_u32(flag, blk.ctypes.data_as(C.POINTER(C.c_uint32)), blk.size, pu8, buf.size,
+                                C.byref(n))
+        assert rc == 0, rc
+
+
+def U_unpack_host(packed, block_off, n, L):
+    out = np.empty(128, dtype=np.uint32)
+    cnt, ovf = C.c_int(0), C.c_int(0)
+    cons = C.c_size_t(0)
+    po = out.ctypes.data_as(C.POINTER(C.c_uint32))
+    for b in range(block_off.size - 1):
+        a, e = int(block_off[b]), int(block_off[b + 1])
+        blk = packed[a:e]
+        rc = L.utl_unpack_u32(blk.ctypes.data_as(C.POINTER(C.c_uint8)), blk.size, po, C.byref(cnt), C.byref(cons),
+                              C.byref(ovf))
+        assert rc == 0, rc
+
+
+def U_get_host(packed, block_off, positions, L):
+    v, ovf = C.c_uint32(0), C.c_int(0)
+    for p in positions:
+        b = int(p) // 128
+        a, e = int(block_off[b]), int(block_off[b + 1])
+        blk = packed[a:e]
+        rc = L.utl_get_u32(int(p) % 128, blk.ctypes.data_as(C.POINTER(C.c_uint8)), blk.size, C.byref(v), C.byref(ovf))
+        assert rc == 0, rc
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -304,10 +487,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--log2n", type=int, default=28, help="values per GPU of the c3 workloads (2^log2n)")
     ap.add_argument("--knob", action="append", default=[], help="kernel knob id=value (see utl_set_knob)")
+    ap.add_argument("--serve-requests", type=int, default=10000, help="c5: requests per offered rate")
+    ap.add_argument("--serve-slots", type=int, default=3, help="c5: batches in flight (CUDA streams)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "c5":
+        return run_serving(args)
 
     import torch
     import torch.distributed as dist

@@ -856,11 +856,6 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
       __syncthreads();
     }
 
-    // the next tile is taken now (its phase A follows phase C); the atomic's
-    // result is only stored at the end of the iteration
-    unsigned long long next_tile = 0;
-    if (tid == 0) next_tile = atomicAdd((unsigned long long*)a.counter, 1ull);
-
     // phase D of t_{i-1}
     if (ptile >= 0) {
       const uint64_t G = S.prefix;
@@ -895,7 +890,8 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
       if (write) quad::quad_write_block(plan, x, kModePlain, 0, S.hb[lb], S.idx[lb], o, j, qm);
       if (direct && tid == 0) S.tile[cb] = -1;  // nothing pending
     }
-    if (tid == 0) S.next = (int64_t)next_tile;
+    // the next tile is taken last: its phase A follows at once
+    if (tid == 0) S.next = (int64_t)atomicAdd((unsigned long long*)a.counter, 1ull);
   }
 }
 
