@@ -256,9 +256,12 @@ UTL_API int utl_unpack_streams_u64(const uint8_t *h_packed, size_t packed_len,
  *   UTL_KNOB_UNPACK_SCHEDULE: 0 = one CTA per 32 blocks, 1 = persistent
  *     warps with the next group's bytes in flight (cp.async double buffer).
  *   UTL_KNOB_PACK_CTAS_PER_SM: cap on resident pack CTAs per SM (0 = the
- *     occupancy maximum). */
+ *     occupancy maximum).
+ *   UTL_KNOB_PACK_SCHEDULE: uint32 pack kernel, 0 = four threads per block
+ *     (CTA tiles), 1 = one thread per block (independent warp tiles). */
 #define UTL_KNOB_UNPACK_SCHEDULE 0
 #define UTL_KNOB_PACK_CTAS_PER_SM 1
+#define UTL_KNOB_PACK_SCHEDULE 2
 UTL_API int utl_set_knob(int knob, int value);
 UTL_API int utl_get_knob(int knob);
 

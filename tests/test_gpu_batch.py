@@ -37,9 +37,19 @@ def sched(request):
     L.utl_set_knob(0, old)
 
 
+@pytest.fixture(params=[0, 1], ids=["pack_quad", "pack_lane"])
+def psched(request):
+    from utlpfor_b200._lib import load
+    L = load()
+    old = L.utl_get_knob(2)
+    assert L.utl_set_knob(2, request.param) == 0
+    yield request.param
+    L.utl_set_knob(2, old)
+
+
 @pytest.mark.parametrize("flag", range(8))
-@pytest.mark.parametrize("kind", ["small", "exc", "dense_exc", "sorted", "walk", "wide", "const"])
-def test_pack_unpack_batch_u32(env, flag, kind, sched):
+@pytest.mark.parametrize("kind", ["small", "exc", "dense_exc", "sorted", "walk", "wide", "const", "zero", "full"])
+def test_pack_unpack_batch_u32(env, flag, kind, sched, psched):
     U, torch = env
     rng = np.random.default_rng(flag * 31 + len(kind))
     vals, vo = streams(rng, LENS, kind)
@@ -86,7 +96,7 @@ def test_pack_unpack_batch_u64(env, flag, kind):
 
 @pytest.mark.parametrize("is64", [False, True])
 @pytest.mark.parametrize("flag", [0, 1, 3, 5])
-def test_get_batch(env, is64, flag):
+def test_get_batch(env, is64, flag, psched):
     U, torch = env
     rng = np.random.default_rng(77 + flag)
     kinds = ("sorted", "exc", "walk", "full") if not is64 else ("for64", "full", "walk")
@@ -154,7 +164,7 @@ def test_host_buffer_streams(env):
         assert np.array_equal(out, vals)
 
 
-def test_large_round_trip_properties(env, sched):
+def test_large_round_trip_properties(env, sched, psched):
     """2^24 values with the exception-heavy shape: pack is byte-identical to
     the oracle (checked by digest), unpack restores every value."""
     U, torch = env

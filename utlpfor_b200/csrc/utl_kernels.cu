@@ -17,6 +17,7 @@
 
 #include "utl_device.cuh"
 #include "utl_launch.h"
+#include "utl_lane.cuh"
 #include "utl_quad.cuh"
 
 namespace utl {
@@ -896,6 +897,255 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
 }
 
 // ------------------------------------------------------------------------
+// Pack, one thread per block: every warp runs on its own over tiles of 32
+// consecutive blocks (no CTA barriers).  A warp takes a tile, loads it
+// (cp.async into 528-byte slots), plans every block (one per thread),
+// scans the lengths and publishes the tile's aggregate at once -- nothing
+// between taking a tile and publishing it waits on another warp.  Then
+// each thread writes its block into the warp's image; the next tile is
+// taken, loaded, planned and published while the look-back loads of the
+// current one are in flight; finally the current tile's look-back is
+// finished and its image streamed to HBM at the resolved offset.
+// ------------------------------------------------------------------------
+constexpr int kLWarps = 1;
+constexpr int kLThreads = kLWarps * 32;
+struct LaneWarpSmem {
+  uint4 in[32 * lane::kSlot / 16];
+  uint4 img[lane::kImage / 16];
+};
+static_assert(lane::kSlot % 16 == 0 && lane::kImage % 16 == 0, "16-byte slots");
+
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Issue the loads of tile `tile` into the slots; returns this lane's block
+// value count (0 past the last block).  Whole, contiguous, 16-byte aligned
+// tiles go through cp.async; others are loaded and zero-padded per block.
+__device__ __forceinline__ int lane_load_tile(const PackArgs& a, int64_t tile, uint8_t* inb, int lane) {
+  const int64_t gb = tile * 32 + lane;
+  uint64_t first = 0;
+  int n = 0;
+  if (gb < a.n_blocks) block_span(a.val_off, a.block_start, a.n_streams, gb, &first, &n);
+  const uint32_t* vals = (const uint32_t*)a.values;
+  const uint64_t f0 = __shfl_sync(kFull, first, 0);
+  const bool ok = n == kBlock && first == f0 + (uint64_t)kBlock * lane;
+  if (__all_sync(kFull, ok) && (((uintptr_t)(vals + f0)) & 15) == 0) {
+    const uint8_t* src = (const uint8_t*)(vals + f0) + 16 * lane;
+    uint8_t* dst = inb + 16 * lane;
+#pragma unroll 8
+    for (int k = 0; k < 32; k++) cp_async16(dst + k * lane::kSlot, src + 512 * k);
+  } else {
+    for (int k = 0; k < 32; k++) {
+      const uint64_t fk = __shfl_sync(kFull, first, k);
+      const int nk = __shfl_sync(kFull, n, k);
+      uint32_t w[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int i = 4 * lane + q;
+        w[q] = i < nk ? __ldcs(vals + fk + i) : 0u;
+      }
+      *(uint4*)(inb + k * lane::kSlot + 16 * lane) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+  cp_async_commit();
+  return n;
+}
+
+// Tile offsets of the lane pack.  Every tile publishes its aggregate (its
+// byte length) twice: in its own word agg[t] (length + 1; 0 = not yet) and
+// added into the word of its group of 32 tiles (sum << 6 | count; the
+// group is complete at count 32).  Nothing is overwritten later.  A warp
+// knows the inclusive prefix of the last tile it packed, so the exclusive
+// prefix of its current tile t is that plus the aggregates of the tiles in
+// between: whole groups by their group words, the ragged ends by the tile
+// words.  All these loads go out at once, one round trip.  Tiles are taken
+// in order and every taken tile is published right after its plan, so
+// every wait ends; waits are still bounded (UTL_ERR_TIMEOUT).
+struct LaneScan {
+  uint32_t* agg;  // n_tiles words
+  uint32_t* grp;  // ceil(n_tiles / 32) words
+};
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void lane_publish(const LaneScan& sc, int64_t t, uint32_t total) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(sc.agg + t), "r"(total + 1u) : "memory");
+  atomicAdd(&sc.grp[t >> 5], (total << 6) | 1u);
+}
+
+// The loads of a window sum over tiles lo < j < t, issued early.
+struct LaneWin {
+  int64_t a, b;      // tiles a..b (a > b: empty)
+  int64_t ga, gb;    // whole groups ga..gb (ga > gb: none)
+  uint32_t head, tail, g0, g1;
+};
+__device__ __forceinline__ void lane_win_issue(const LaneScan& sc, int64_t lo, int64_t t, int lane, LaneWin& w) {
+  w.a = lo + 1;
+  w.b = t - 1;
+  w.ga = (w.a + 31) >> 5;
+  w.gb = ((w.b + 1) >> 5) - 1;
+  if (w.ga > w.gb) {  // no whole group: every tile on its own (at most 62)
+    w.ga = 1;
+    w.gb = 0;
+  }
+  const bool groups = w.ga <= w.gb;
+  const int64_t head_end = groups ? 32 * w.ga - 1 : w.b;     // last head tile
+  const int64_t tail_beg = groups ? 32 * (w.gb + 1) : w.b + 1;
+  const int64_t h = w.a + lane, h2 = w.a + 32 + lane, tl = tail_beg + lane;
+  // head tiles a..head_end (up to 62 without groups: two per lane)
+  w.head = (w.a <= w.b && h <= head_end) ? ld_relaxed_u32(sc.agg + h) : 1u;
+  w.tail = (!groups && h2 <= head_end) ? ld_relaxed_u32(sc.agg + h2)
+                                       : ((groups && tl <= w.b) ? ld_relaxed_u32(sc.agg + tl) : 1u);
+  w.g0 = (groups && w.ga + lane <= w.gb) ? ld_relaxed_u32(sc.grp + w.ga + lane) : 32u;
+  w.g1 = (groups && w.ga + 32 + lane <= w.gb) ? ld_relaxed_u32(sc.grp + w.ga + 32 + lane) : 32u;
+}
+__device__ __forceinline__ uint32_t lane_wait_tile(const LaneScan& sc, int64_t j, uint32_t v, bool& to) {
+  for (uint32_t it = 0; v == 0; it++) {
+    if (it > kSpinLimit) {
+      to = true;
+      return 1u;
+    }
+    __nanosleep(64);
+    v = ld_relaxed_u32(sc.agg + j);
+  }
+  return v;
+}
+__device__ __forceinline__ uint32_t lane_wait_group(const LaneScan& sc, int64_t g, uint32_t v, bool& to) {
+  for (uint32_t it = 0; (v & 63u) != 32u; it++) {
+    if (it > kSpinLimit) {
+      to = true;
+      return 32u;
+    }
+    __nanosleep(64);
+    v = ld_relaxed_u32(sc.grp + g);
+  }
+  return v;
+}
+// Sum of the window issued by lane_win_issue (whole warp).
+__device__ __forceinline__ uint64_t lane_win_finish(const LaneScan& sc, LaneWin& w, int lane, uint32_t* err) {
+  if (w.a > w.b) return 0;
+  bool to = false;
+  const bool groups = w.ga <= w.gb;
+  const int64_t head_end = groups ? 32 * w.ga - 1 : w.b;
+  const int64_t tail_beg = groups ? 32 * (w.gb + 1) : w.b + 1;
+  const int64_t h = w.a + lane, h2 = w.a + 32 + lane, tl = tail_beg + lane;
+  uint64_t sum = 0;
+  if (h <= head_end) sum += lane_wait_tile(sc, h, w.head, to) - 1u;
+  if (!groups && h2 <= head_end) sum += lane_wait_tile(sc, h2, w.tail, to) - 1u;
+  if (groups && tl <= w.b) sum += lane_wait_tile(sc, tl, w.tail, to) - 1u;
+  if (groups) {
+    if (w.ga + lane <= w.gb) sum += lane_wait_group(sc, w.ga + lane, w.g0, to) >> 6;
+    if (w.ga + 32 + lane <= w.gb) sum += lane_wait_group(sc, w.ga + 32 + lane, w.g1, to) >> 6;
+    for (int64_t g = w.ga + 64 + lane; g <= w.gb; g += 32)  // very wide windows
+      sum += lane_wait_group(sc, g, ld_relaxed_u32(sc.grp + g), to) >> 6;
+  }
+  if (__any_sync(kFull, to) && lane == 0 && err) atomicOr(err, 1u << 10);
+  return warp_sum_u64(sum);
+}
+
+// Take a tile, load it, plan its blocks and publish its aggregate.
+template <bool DELTA>
+__device__ __forceinline__ void lane_take_and_plan(const PackArgs& a, const LaneScan& sc, uint8_t* inb, uint4* slot,
+                                                   int lane, int64_t& t, int& n, lane::Plan& p, int& incl,
+                                                   int& total) {
+  unsigned long long tv = 0;
+  if (lane == 0) tv = atomicAdd((unsigned long long*)a.counter, 1ull);
+  t = (int64_t)__shfl_sync(kFull, tv, 0);
+  if (t >= a.n_tiles) return;
+  n = lane_load_tile(a, t, inb, lane);
+  cp_async_wait0();
+  __syncwarp();
+  p.len = 0;
+  p.exc = 0;
+  if (n > 0) p = lane::plan_block<DELTA>(slot, n, a.flag);
+  incl = warp_incl_scan(p.len, lane);
+  total = __shfl_sync(kFull, incl, 31);
+  if (lane == 31) lane_publish(sc, t, (uint32_t)total);
+}
+
+template <bool DELTA>
+__device__ __forceinline__ void lane_write(const lane::Plan& p, const uint4* slot, uint8_t* o) {
+  if (__any_sync(__activemask(), p.exc > 0)) lane::write_block<DELTA, true>(p, slot, o);
+  else lane::write_block<DELTA, false>(p, slot, o);
+}
+
+template <bool DELTA>
+__global__ void __launch_bounds__(kLThreads) pack_lane_kernel(PackArgs a) {
+  extern __shared__ uint4 smem4[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  LaneWarpSmem& W = ((LaneWarpSmem*)smem4)[warp];
+  uint8_t* inb = (uint8_t*)W.in;
+  uint8_t* img = (uint8_t*)W.img;
+  uint4* slot = (uint4*)(inb + lane * lane::kSlot);
+
+  LaneScan sc;
+  sc.agg = (uint32_t*)a.tile_status;
+  sc.grp = sc.agg + a.n_tiles;
+  int64_t prev = -1;      // the last tile this warp packed
+  uint64_t prev_incl = 0;  // its inclusive prefix
+  int64_t tile;
+  int n = 0, incl = 0, total = 0;
+  lane::Plan p;
+  lane_take_and_plan<DELTA>(a, sc, inb, slot, lane, tile, n, p, incl, total);
+  while (tile < a.n_tiles) {
+    const int off = incl - p.len;
+    const int64_t gb = tile * 32 + lane;
+    // blocks are a prefix of the lanes; their start offsets pick the rounds
+    const unsigned act = __ballot_sync(kFull, n > 0);
+    const int last = act ? 31 - __clz(act) : 0;
+    const int n_rounds = act ? __shfl_sync(kFull, off, last) / lane::kWindow + 1 : 0;
+    LaneWin win;
+    lane_win_issue(sc, prev, tile, lane, win);
+    if (n_rounds <= 1) {
+      if (n > 0) lane_write<DELTA>(p, slot, img + off);
+      __syncwarp();
+      const int64_t cur = tile;
+      const int cur_n = n, cur_off = off, cur_incl = incl, cur_total = total;
+      // the slots are free: the next tile is taken, loaded, planned and
+      // published while this tile's window loads are in flight
+      lane_take_and_plan<DELTA>(a, sc, inb, slot, lane, tile, n, p, incl, total);
+
+      const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
+      if (G + (uint64_t)cur_total <= a.out_cap) image_copy_out(W.img, 0, cur_total, a.out, G, lane);
+      else if (lane == 0 && a.err) atomicOr(a.err, 1u << 9);
+      const int64_t cgb = cur * 32 + lane;
+      if (cur_n > 0) {
+        a.block_off[cgb] = G + (uint64_t)cur_off;
+        if (cgb == a.n_blocks - 1) a.block_off[a.n_blocks] = G + (uint64_t)cur_incl;
+      }
+      prev = cur;
+      prev_incl = G + (uint64_t)cur_total;
+      __syncwarp();
+    } else {
+      // a tile larger than the image: its offset first, then one window of
+      // blocks at a time is written and streamed out
+      const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
+      const bool fits = G + (uint64_t)total <= a.out_cap;
+      if (!fits && lane == 0 && a.err) atomicOr(a.err, 1u << 9);
+      const int my_round = n > 0 ? off / lane::kWindow : -1;
+      for (int r = 0; r < n_rounds; r++) {
+        const unsigned in_r = __ballot_sync(kFull, my_round == r);
+        const unsigned in_next = __ballot_sync(kFull, my_round == r + 1);
+        const int base = __shfl_sync(kFull, off, __ffs(in_r) - 1);
+        const int end = in_next ? __shfl_sync(kFull, off, __ffs(in_next) - 1) : total;
+        if (my_round == r) lane_write<DELTA>(p, slot, img + (off - base));
+        __syncwarp();
+        if (fits) image_copy_out(W.img, 0, end - base, a.out, G + (uint64_t)base, lane);
+        __syncwarp();
+      }
+      if (n > 0) {
+        a.block_off[gb] = G + (uint64_t)off;
+        if (gb == a.n_blocks - 1) a.block_off[a.n_blocks] = G + (uint64_t)incl;
+      }
+      prev = tile;
+      prev_incl = G + (uint64_t)total;
+      lane_take_and_plan<DELTA>(a, sc, inb, slot, lane, tile, n, p, incl, total);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
 // Get: one thread per query; queries that need the reference's full-block
 // fallback (delta blocks, deep positions) are resolved by the whole warp.
 // ------------------------------------------------------------------------
@@ -1226,7 +1476,35 @@ static int g_pipe_ctas = 0;
 static int g_unpack_schedule = 1;
 static int g_pack_cap = 0;
 
+static int g_pack_schedule = 1;
+static int g_lane_pack_ctas = 0;
+
+static cudaError_t pack_lane(const PackArgs& a_in, cudaStream_t st) {
+  PackArgs a = a_in;
+  a.n_tiles = (a.n_blocks + 31) / 32;
+  const size_t smem = sizeof(LaneWarpSmem) * kLWarps;
+  if (g_lane_pack_ctas == 0) {
+    for (int d = 0; d < 2; d++) {
+      const void* f = d ? (const void*)pack_lane_kernel<true> : (const void*)pack_lane_kernel<false>;
+      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_lane_pack_ctas, pack_lane_kernel<false>, kLThreads, smem);
+    if (g_lane_pack_ctas <= 0) g_lane_pack_ctas = 1;
+  }
+  const int per_sm = (g_pack_cap > 0 && g_pack_cap < g_lane_pack_ctas) ? g_pack_cap : g_lane_pack_ctas;
+  int64_t grid = (int64_t)num_sms() * per_sm;
+  if (grid * kLWarps > a.n_tiles) grid = (a.n_tiles + kLWarps - 1) / kLWarps;
+  if (grid < 1) grid = 1;
+  if (a.flag & kDelta) pack_lane_kernel<true><<<(unsigned)grid, kLThreads, smem, st>>>(a);
+  else pack_lane_kernel<false><<<(unsigned)grid, kLThreads, smem, st>>>(a);
+  note_launch(1);
+  return cudaGetLastError();
+}
+
 cudaError_t pack(bool u64, const PackArgs& a_in, cudaStream_t st) {
+  if (!u64 && g_pack_schedule == 1) return pack_lane(a_in, st);
   if (!u64) {
     PackArgs a = a_in;
     a.n_tiles = (a.n_blocks + kQTile - 1) / kQTile;
@@ -1363,6 +1641,10 @@ int set_knob(int knob, int value) {
       if (value < 0 || value > 32) return -1;
       g_pack_cap = value;
       return 0;
+    case 2:  // UTL_KNOB_PACK_SCHEDULE
+      if (value != 0 && value != 1) return -1;
+      g_pack_schedule = value;
+      return 0;
   }
   return -1;
 }
@@ -1370,6 +1652,7 @@ int get_knob(int knob) {
   switch (knob) {
     case 0: return g_unpack_schedule;
     case 1: return g_pack_cap;
+    case 2: return g_pack_schedule;
   }
   return -1;
 }

@@ -6,6 +6,7 @@ utlpfor_b200/tuned/<gpu name>.json; apply() loads that file (if any) for
 the current GPU and sets the knobs.  Knobs (include/utlpfor.h):
   0 UTL_KNOB_UNPACK_SCHEDULE   0 tiles, 1 persistent pipelined
   1 UTL_KNOB_PACK_CTAS_PER_SM  0 occupancy maximum, else a cap
+  2 UTL_KNOB_PACK_SCHEDULE     0 four threads per block, 1 one thread per block
 
     python -m utlpfor_b200.tune [--log2n 26]
 """
@@ -18,7 +19,7 @@ from ._lib import load
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 TUNED = os.path.join(HERE, "tuned")
-CANDIDATES = {0: [0, 1], 1: [0, 3, 2]}
+CANDIDATES = {0: [0, 1], 2: [1, 0], 1: [0, 3, 2]}  # pack schedule before its CTA cap
 
 
 def _gpu_name(torch, dev=None):
@@ -73,6 +74,7 @@ def tune(log2n=26, flag=0, write=True):
     out = torch.empty_like(v)
     codec.pack(v)
     best, results = {}, {}
+    ref = None
     for knob, cands in CANDIDATES.items():
         times = {}
         for c in cands:
@@ -84,6 +86,12 @@ def tune(log2n=26, flag=0, write=True):
                 assert torch.equal(out, v), "unpack schedule %d gave wrong values" % c
             else:
                 t = _time(lambda: codec.pack(v), torch)
+                codec.pack(v)
+                torch.cuda.synchronize()
+                got = codec.packed[:codec.packed_len].clone()
+                if ref is None:
+                    ref = got
+                assert torch.equal(got, ref), "pack knob %d=%d changed the packed bytes" % (knob, c)
             times[c] = t
         pick = min(times, key=times.get)
         L.utl_set_knob(knob, pick)
