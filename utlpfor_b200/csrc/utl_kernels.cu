@@ -915,6 +915,10 @@ struct LaneWarpSmem {
 };
 static_assert(lane::kSlot % 16 == 0 && lane::kImage % 16 == 0, "16-byte slots");
 
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Issue the loads of tile `tile` into the slots; returns this lane's block
@@ -934,16 +938,22 @@ __device__ __forceinline__ int lane_load_tile(const PackArgs& a, int64_t tile, u
 #pragma unroll 8
     for (int k = 0; k < 32; k++) cp_async16(dst + k * lane::kSlot, src + 512 * k);
   } else {
+    // block by block: whole 16-byte aligned blocks in 16-byte copies, the
+    // others value by value; positions past the block's count are zeroed
     for (int k = 0; k < 32; k++) {
       const uint64_t fk = __shfl_sync(kFull, first, k);
       const int nk = __shfl_sync(kFull, n, k);
-      uint32_t w[4];
+      uint8_t* dst = inb + k * lane::kSlot + 16 * lane;
+      const uint32_t* src = vals + fk + 4 * lane;
+      if (nk == kBlock && (((uintptr_t)(vals + fk)) & 15) == 0) {
+        cp_async16(dst, src);
+      } else {
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int i = 4 * lane + q;
-        w[q] = i < nk ? __ldcs(vals + fk + i) : 0u;
+        for (int q = 0; q < 4; q++) {
+          if (4 * lane + q < nk) cp_async4(dst + 4 * q, src + q);
+          else *(uint32_t*)(dst + 4 * q) = 0u;
+        }
       }
-      *(uint4*)(inb + k * lane::kSlot + 16 * lane) = make_uint4(w[0], w[1], w[2], w[3]);
     }
   }
   cp_async_commit();
@@ -1064,6 +1074,52 @@ __device__ __forceinline__ void lane_take_and_plan(const PackArgs& a, const Lane
   if (lane == 31) lane_publish(sc, t, (uint32_t)total);
 }
 
+// out[G + r] = img[r] for r in [0, len): whole aligned 16-byte chunks of
+// the destination, each assembled from two aligned 16-byte image loads and
+// a funnel shift by the (warp-uniform) misalignment; the partial chunks at
+// the two ends bytewise.  The image has 32 readable bytes past len.
+__device__ __forceinline__ void lane_copy_out(const uint4* img4, int len, uint8_t* out, uint64_t G, int lane) {
+  if (len <= 0) return;
+  const uint8_t* img = (const uint8_t*)img4;
+  const uint64_t A0 = (uint64_t)(uintptr_t)out + G;
+  const uint64_t c0 = A0 >> 4, c1 = (A0 + (uint64_t)len + 15) >> 4;
+  const int s = (int)((0u - (uint32_t)A0) & 15u);  // image offset of every chunk, mod 16
+  const int q = s >> 2, b = (s & 3) * 8;
+  for (uint64_t c = c0 + lane; c < c1; c += 32) {
+    const int64_t o = (int64_t)(c * 16 - A0);
+    uint8_t* gp = (uint8_t*)(uintptr_t)(c * 16);
+    if (o >= 0 && o + 16 <= len) {
+      const int ob = (int)(o >> 4);
+      const uint4 I0 = img4[ob], I1 = img4[ob + 1];
+      uint32_t v0, v1, v2, v3, v4;
+      switch (q) {
+        case 0: v0 = I0.x; v1 = I0.y; v2 = I0.z; v3 = I0.w; v4 = I1.x; break;
+        case 1: v0 = I0.y; v1 = I0.z; v2 = I0.w; v3 = I1.x; v4 = I1.y; break;
+        case 2: v0 = I0.z; v1 = I0.w; v2 = I1.x; v3 = I1.y; v4 = I1.z; break;
+        default: v0 = I0.w; v1 = I1.x; v2 = I1.y; v3 = I1.z; v4 = I1.w; break;
+      }
+      __stcs((uint4*)gp, make_uint4(__funnelshift_r(v0, v1, b), __funnelshift_r(v1, v2, b),
+                                    __funnelshift_r(v2, v3, b), __funnelshift_r(v3, v4, b)));
+    } else {
+      // a chunk shared with the neighbouring tiles: its four words, whole
+      // where they lie inside [0, len), else byte by byte
+#pragma unroll
+      for (int wq = 0; wq < 4; wq++) {
+        const int64_t io = o + 4 * wq;
+        if (io >= 0 && io + 4 <= len) {
+          const uint32_t* iw = (const uint32_t*)img4;
+          const int ia = (int)io;
+          *(uint32_t*)(gp + 4 * wq) = __funnelshift_r(iw[ia >> 2], iw[(ia >> 2) + 1], (ia & 3) * 8);
+        } else if (io + 4 > 0 && io < len) {
+#pragma unroll
+          for (int bb = 0; bb < 4; bb++)
+            if (io + bb >= 0 && io + bb < len) gp[4 * wq + bb] = img[io + bb];
+        }
+      }
+    }
+  }
+}
+
 template <bool DELTA>
 __device__ __forceinline__ void lane_write(const lane::Plan& p, const uint4* slot, uint8_t* o) {
   if (__any_sync(__activemask(), p.exc > 0)) lane::write_block<DELTA, true>(p, slot, o);
@@ -1082,7 +1138,7 @@ __global__ void __launch_bounds__(kLThreads) pack_lane_kernel(PackArgs a) {
   LaneScan sc;
   sc.agg = (uint32_t*)a.tile_status;
   sc.grp = sc.agg + a.n_tiles;
-  int64_t prev = -1;      // the last tile this warp packed
+  int64_t prev = -1;       // the last tile this warp packed
   uint64_t prev_incl = 0;  // its inclusive prefix
   int64_t tile;
   int n = 0, incl = 0, total = 0;
@@ -1107,7 +1163,7 @@ __global__ void __launch_bounds__(kLThreads) pack_lane_kernel(PackArgs a) {
       lane_take_and_plan<DELTA>(a, sc, inb, slot, lane, tile, n, p, incl, total);
 
       const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
-      if (G + (uint64_t)cur_total <= a.out_cap) image_copy_out(W.img, 0, cur_total, a.out, G, lane);
+      if (G + (uint64_t)cur_total <= a.out_cap) lane_copy_out(W.img, cur_total, a.out, G, lane);
       else if (lane == 0 && a.err) atomicOr(a.err, 1u << 9);
       const int64_t cgb = cur * 32 + lane;
       if (cur_n > 0) {
@@ -1131,7 +1187,7 @@ __global__ void __launch_bounds__(kLThreads) pack_lane_kernel(PackArgs a) {
         const int end = in_next ? __shfl_sync(kFull, off, __ffs(in_next) - 1) : total;
         if (my_round == r) lane_write<DELTA>(p, slot, img + (off - base));
         __syncwarp();
-        if (fits) image_copy_out(W.img, 0, end - base, a.out, G + (uint64_t)base, lane);
+        if (fits) lane_copy_out(W.img, end - base, a.out, G + (uint64_t)base, lane);
         __syncwarp();
       }
       if (n > 0) {

@@ -153,13 +153,16 @@ __device__ __forceinline__ void raw_stats(const uint4* s4, uint32_t& mn, uint32_
 #pragma unroll
     for (int q = 0; q < 4; q++) t[q] = s4[4 * c8 + q];
     if (MM) {
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        mn = __vimin3_u32(mn, t[q].x, t[q].y);
-        mn = __vimin3_u32(mn, t[q].z, t[q].w);
-        mx = __vimax3_u32(mx, t[q].x, t[q].y);
-        mx = __vimax3_u32(mx, t[q].z, t[q].w);
-      }
+      const uint32_t m01 = __vimin3_u32(__vimin3_u32(t[0].x, t[0].y, t[0].z), t[0].w, t[1].x);
+      const uint32_t m23 = __vimin3_u32(__vimin3_u32(t[2].x, t[2].y, t[2].z), t[2].w, t[3].x);
+      const uint32_t n01 = __vimin3_u32(t[1].y, t[1].z, t[1].w);
+      const uint32_t n23 = __vimin3_u32(t[3].y, t[3].z, t[3].w);
+      mn = __vimin3_u32(mn, __vimin3_u32(m01, m23, n01), n23);
+      const uint32_t x01 = __vimax3_u32(__vimax3_u32(t[0].x, t[0].y, t[0].z), t[0].w, t[1].x);
+      const uint32_t x23 = __vimax3_u32(__vimax3_u32(t[2].x, t[2].y, t[2].z), t[2].w, t[3].x);
+      const uint32_t y01 = __vimax3_u32(t[1].y, t[1].z, t[1].w);
+      const uint32_t y23 = __vimax3_u32(t[3].y, t[3].z, t[3].w);
+      mx = __vimax3_u32(mx, __vimax3_u32(x01, x23, y01), y23);
     }
     if (HI) {
       const uint32_t a0 = nib(t[0].x) + nib(t[0].y) + nib(t[0].z) + nib(t[0].w) + nib(t[1].x) + nib(t[1].y) +
@@ -277,6 +280,33 @@ __device__ __forceinline__ void put_seg(uint32_t* pw, int d4, int sh, int w, int
   if (d4 >= 3) b[18] = (uint8_t)(x[3] >> (sh + 16));
 }
 
+// The payload words of lanes 4g..4g+3 at width BW (scalar.go:7-59): lane
+// k's eight work values, masked to BW bits, packed LSB first into BW/4
+// words; word w of the four lanes is one 16-byte segment.  The bit
+// positions are constants, so each value costs a mask and a shift-or.
+template <int BW>
+__device__ __forceinline__ void pack_group(const uint32_t (&w)[8][4], uint32_t* pw, int d4, int sh, int g) {
+  constexpr int NW = BW / 4;
+  constexpr uint32_t MASK = BW >= 32 ? 0xFFFFFFFFu : ((1u << (BW & 31)) - 1u);
+  uint32_t x[NW][4];
+#pragma unroll
+  for (int i = 0; i < NW; i++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) x[i][k] = 0;
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    const int pos = r * BW, wi = pos >> 5, s = pos & 31;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint32_t m = w[r][k] & MASK;
+      x[wi][k] |= m << s;
+      if (s + BW > 32) x[wi + 1][k] |= m >> (32 - s);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NW; i++) put_seg(pw, d4, sh, i, g, x[i]);
+}
+
 // Write the block at o (shared memory): header, StreamVByte length, FOR
 // base, the UTL payload (scalar.go:7-59: lane L's eight values packed LSB
 // first into bw/4 words, word w of lane L at byte 64w + 4L), then the
@@ -292,7 +322,7 @@ __device__ void write_block(const Plan& p, const uint4* s4, uint8_t* o) {
   if (p.forb) put_bytes(o + m, p.base, p.forb);
   const int bw = p.bw;
   uint8_t* pay = o + p.p_off;
-  const uint32_t mask = bw >= 32 ? 0xFFFFFFFFu : ((1u << bw) - 1u);
+  const uint32_t mask = bw >= 32 ? 0xFFFFFFFFu : ((1u << bw) - 1u);  // exceptions are above it
   const int d4 = (int)((uintptr_t)pay & 3);
   uint32_t* pw = (uint32_t*)(pay - d4);
   const int sh = 32 - 8 * d4;
@@ -311,27 +341,16 @@ __device__ void write_block(const Plan& p, const uint4* s4, uint8_t* o) {
 #pragma unroll
       for (int q = 0; q < 4; q++) bm[q] |= f[q] << (4 * g);
     }
-    uint32_t lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
-    int bits = 0, wi = 0;
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const uint32_t mk = w[r][k] & mask;
-        lo[k] |= mk << bits;
-        hi[k] |= __funnelshift_l(mk, 0u, bits);
-      }
-      bits += bw;
-      if (bits >= 32) {
-        put_seg(pw, d4, sh, wi, g, lo);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          lo[k] = hi[k];
-          hi[k] = 0;
-        }
-        bits -= 32;
-        wi++;
-      }
+    switch (bw) {
+      case 4: pack_group<4>(w, pw, d4, sh, g); break;
+      case 8: pack_group<8>(w, pw, d4, sh, g); break;
+      case 12: pack_group<12>(w, pw, d4, sh, g); break;
+      case 16: pack_group<16>(w, pw, d4, sh, g); break;
+      case 20: pack_group<20>(w, pw, d4, sh, g); break;
+      case 24: pack_group<24>(w, pw, d4, sh, g); break;
+      case 28: pack_group<28>(w, pw, d4, sh, g); break;
+      case 32: pack_group<32>(w, pw, d4, sh, g); break;
+      default: break;  // bw 0: no payload
     }
   }
   if (EXC && p.exc) {
