@@ -580,10 +580,16 @@ def main():
     traffic = profiled_traffic()
     dom = "pack" if pack_ms >= unpack_ms else "unpack"
     dom_achieved = pack_gbs if dom == "pack" else unpack_gbs
-    dom_traffic = traffic.get(dom)
+    if is64:
+        kname = {"pack": "pack_kernel", "unpack": "unpack_kernel"}[dom]
+    elif dom == "pack":
+        kname = "pack_lane_kernel" if L.utl_get_knob(2) == 1 else "pack_quad_kernel"
+    else:
+        kname = "unpack_quad_pipe_kernel" if L.utl_get_knob(0) == 1 else "unpack_quad_kernel"
+    dom_traffic = traffic.get(kname)
     roofline = {"bound": "hbm", "achieved": dom_achieved, "peak": peak, "unit": "GB/s",
                 "frac": dom_achieved / peak, "traffic": (dom_traffic * n) if dom_traffic else None,
-                "kernel": dom + "_kernel", "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
+                "kernel": kname, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6650 GB/s",
                 "algorithmic_bytes": pack_bytes if dom == "pack" else unpack_bytes}
 

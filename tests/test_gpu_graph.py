@@ -37,5 +37,5 @@ def test_graph_replay_matches_eager():
 
 def test_tuner_candidates_agree():
     from utlpfor_b200.tune import tune
-    cfg = tune(log2n=18, write=False)
-    assert set(cfg["knobs"]) == {"0", "1"}
+    cfg = tune(log2n=18, write=False)  # asserts that every pack candidate gives the same bytes
+    assert set(cfg["knobs"]) == {"0", "1", "2"}

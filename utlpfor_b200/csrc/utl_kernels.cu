@@ -1134,70 +1134,73 @@ __global__ void __launch_bounds__(kLThreads) pack_lane_kernel(PackArgs a) {
   uint8_t* inb = (uint8_t*)W.in;
   uint8_t* img = (uint8_t*)W.img;
   uint4* slot = (uint4*)(inb + lane * lane::kSlot);
-
   LaneScan sc;
   sc.agg = (uint32_t*)a.tile_status;
   sc.grp = sc.agg + a.n_tiles;
-  int64_t prev = -1;       // the last tile this warp packed
+  int64_t prev = -1;       // the last tile this warp finished
   uint64_t prev_incl = 0;  // its inclusive prefix
-  int64_t tile;
-  int n = 0, incl = 0, total = 0;
+  // the current tile (planned and published; -1: none yet) and its layout
+  int64_t cur = -1;
+  int n = 0, incl = 0, total = 0, n_rounds = 0;
   lane::Plan p;
-  lane_take_and_plan<DELTA>(a, sc, inb, slot, lane, tile, n, p, incl, total);
-  while (tile < a.n_tiles) {
+  p.len = 0;
+  LaneWin win;
+  for (;;) {
     const int off = incl - p.len;
-    const int64_t gb = tile * 32 + lane;
+    if (cur >= 0) {
+      lane_win_issue(sc, prev, cur, lane, win);
+      if (n_rounds <= 1) {
+        if (n > 0) lane_write<DELTA>(p, slot, img + off);
+      } else {
+        // a tile larger than the image: its offset first, then one window
+        // of blocks at a time is written and streamed out
+        const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
+        const bool fits = G + (uint64_t)total <= a.out_cap;
+        if (!fits && lane == 0 && a.err) atomicOr(a.err, 1u << 9);
+        const int my_round = n > 0 ? off / lane::kWindow : -1;
+        for (int r = 0; r < n_rounds; r++) {
+          const unsigned in_r = __ballot_sync(kFull, my_round == r);
+          const unsigned in_next = __ballot_sync(kFull, my_round == r + 1);
+          const int base = __shfl_sync(kFull, off, __ffs(in_r) - 1);
+          const int end = in_next ? __shfl_sync(kFull, off, __ffs(in_next) - 1) : total;
+          if (my_round == r) lane_write<DELTA>(p, slot, img + (off - base));
+          __syncwarp();
+          if (fits) lane_copy_out(W.img, end - base, a.out, G + (uint64_t)base, lane);
+          __syncwarp();
+        }
+        const int64_t gb = cur * 32 + lane;
+        if (n > 0) {
+          a.block_off[gb] = G + (uint64_t)off;
+          if (gb == a.n_blocks - 1) a.block_off[a.n_blocks] = G + (uint64_t)incl;
+        }
+        prev = cur;
+        prev_incl = G + (uint64_t)total;
+      }
+      __syncwarp();
+    }
+    // the slots are free: the next tile is taken, loaded, planned and
+    // published while the current tile's window loads are in flight
+    const int64_t done = cur;
+    const int d_n = n, d_off = off, d_incl = incl, d_total = total, d_rounds = n_rounds;
+    lane_take_and_plan<DELTA>(a, sc, inb, slot, lane, cur, n, p, incl, total);
+    if (done >= 0 && d_rounds <= 1) {
+      const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
+      if (G + (uint64_t)d_total <= a.out_cap) lane_copy_out(W.img, d_total, a.out, G, lane);
+      else if (lane == 0 && a.err) atomicOr(a.err, 1u << 9);
+      const int64_t gb = done * 32 + lane;
+      if (d_n > 0) {
+        a.block_off[gb] = G + (uint64_t)d_off;
+        if (gb == a.n_blocks - 1) a.block_off[a.n_blocks] = G + (uint64_t)d_incl;
+      }
+      prev = done;
+      prev_incl = G + (uint64_t)d_total;
+      __syncwarp();
+    }
+    if (cur >= a.n_tiles) break;
     // blocks are a prefix of the lanes; their start offsets pick the rounds
     const unsigned act = __ballot_sync(kFull, n > 0);
     const int last = act ? 31 - __clz(act) : 0;
-    const int n_rounds = act ? __shfl_sync(kFull, off, last) / lane::kWindow + 1 : 0;
-    LaneWin win;
-    lane_win_issue(sc, prev, tile, lane, win);
-    if (n_rounds <= 1) {
-      if (n > 0) lane_write<DELTA>(p, slot, img + off);
-      __syncwarp();
-      const int64_t cur = tile;
-      const int cur_n = n, cur_off = off, cur_incl = incl, cur_total = total;
-      // the slots are free: the next tile is taken, loaded, planned and
-      // published while this tile's window loads are in flight
-      lane_take_and_plan<DELTA>(a, sc, inb, slot, lane, tile, n, p, incl, total);
-
-      const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
-      if (G + (uint64_t)cur_total <= a.out_cap) lane_copy_out(W.img, cur_total, a.out, G, lane);
-      else if (lane == 0 && a.err) atomicOr(a.err, 1u << 9);
-      const int64_t cgb = cur * 32 + lane;
-      if (cur_n > 0) {
-        a.block_off[cgb] = G + (uint64_t)cur_off;
-        if (cgb == a.n_blocks - 1) a.block_off[a.n_blocks] = G + (uint64_t)cur_incl;
-      }
-      prev = cur;
-      prev_incl = G + (uint64_t)cur_total;
-      __syncwarp();
-    } else {
-      // a tile larger than the image: its offset first, then one window of
-      // blocks at a time is written and streamed out
-      const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
-      const bool fits = G + (uint64_t)total <= a.out_cap;
-      if (!fits && lane == 0 && a.err) atomicOr(a.err, 1u << 9);
-      const int my_round = n > 0 ? off / lane::kWindow : -1;
-      for (int r = 0; r < n_rounds; r++) {
-        const unsigned in_r = __ballot_sync(kFull, my_round == r);
-        const unsigned in_next = __ballot_sync(kFull, my_round == r + 1);
-        const int base = __shfl_sync(kFull, off, __ffs(in_r) - 1);
-        const int end = in_next ? __shfl_sync(kFull, off, __ffs(in_next) - 1) : total;
-        if (my_round == r) lane_write<DELTA>(p, slot, img + (off - base));
-        __syncwarp();
-        if (fits) lane_copy_out(W.img, end - base, a.out, G + (uint64_t)base, lane);
-        __syncwarp();
-      }
-      if (n > 0) {
-        a.block_off[gb] = G + (uint64_t)off;
-        if (gb == a.n_blocks - 1) a.block_off[a.n_blocks] = G + (uint64_t)incl;
-      }
-      prev = tile;
-      prev_incl = G + (uint64_t)total;
-      lane_take_and_plan<DELTA>(a, sc, inb, slot, lane, tile, n, p, incl, total);
-    }
+    n_rounds = act ? __shfl_sync(kFull, incl - p.len, last) / lane::kWindow + 1 : 0;
   }
 }
 
