@@ -1074,49 +1074,40 @@ __device__ __forceinline__ void lane_take_and_plan(const PackArgs& a, const Lane
   if (lane == 31) lane_publish(sc, t, (uint32_t)total);
 }
 
-// out[G + r] = img[r] for r in [0, len): whole aligned 16-byte chunks of
-// the destination, each assembled from two aligned 16-byte image loads and
-// a funnel shift by the (warp-uniform) misalignment; the partial chunks at
-// the two ends bytewise.  The image has 32 readable bytes past len.
+// out[G + r] = img[r] for r in [0, len).  The destination's aligned 16-byte
+// chunks start at image offset s + 16i (s = the misalignment, the same for
+// the whole tile); each is assembled from the two aligned image chunks i
+// and i+1 with a funnel shift (a loop per word shift Q).  The bytes before
+// the first and after the last whole chunk (fewer than 16 each) are shared
+// with the neighbouring tiles and go out one byte per lane.  The image has
+// 32 readable bytes past len.
+template <int Q>
+__device__ __forceinline__ void lane_copy_chunks(const uint4* img4, uint4* dst, int nf, int b, int lane) {
+  for (int i = lane; i < nf; i += 32) {
+    const uint4 I0 = img4[i], I1 = img4[i + 1];
+    const uint32_t v[8] = {I0.x, I0.y, I0.z, I0.w, I1.x, I1.y, I1.z, I1.w};
+    __stcs(dst + i, make_uint4(__funnelshift_r(v[Q], v[Q + 1], b), __funnelshift_r(v[Q + 1], v[Q + 2], b),
+                               __funnelshift_r(v[Q + 2], v[Q + 3], b), __funnelshift_r(v[Q + 3], v[Q + 4], b)));
+  }
+}
 __device__ __forceinline__ void lane_copy_out(const uint4* img4, int len, uint8_t* out, uint64_t G, int lane) {
   if (len <= 0) return;
   const uint8_t* img = (const uint8_t*)img4;
-  const uint64_t A0 = (uint64_t)(uintptr_t)out + G;
-  const uint64_t c0 = A0 >> 4, c1 = (A0 + (uint64_t)len + 15) >> 4;
-  const int s = (int)((0u - (uint32_t)A0) & 15u);  // image offset of every chunk, mod 16
-  const int q = s >> 2, b = (s & 3) * 8;
-  for (uint64_t c = c0 + lane; c < c1; c += 32) {
-    const int64_t o = (int64_t)(c * 16 - A0);
-    uint8_t* gp = (uint8_t*)(uintptr_t)(c * 16);
-    if (o >= 0 && o + 16 <= len) {
-      const int ob = (int)(o >> 4);
-      const uint4 I0 = img4[ob], I1 = img4[ob + 1];
-      uint32_t v0, v1, v2, v3, v4;
-      switch (q) {
-        case 0: v0 = I0.x; v1 = I0.y; v2 = I0.z; v3 = I0.w; v4 = I1.x; break;
-        case 1: v0 = I0.y; v1 = I0.z; v2 = I0.w; v3 = I1.x; v4 = I1.y; break;
-        case 2: v0 = I0.z; v1 = I0.w; v2 = I1.x; v3 = I1.y; v4 = I1.z; break;
-        default: v0 = I0.w; v1 = I1.x; v2 = I1.y; v3 = I1.z; v4 = I1.w; break;
-      }
-      __stcs((uint4*)gp, make_uint4(__funnelshift_r(v0, v1, b), __funnelshift_r(v1, v2, b),
-                                    __funnelshift_r(v2, v3, b), __funnelshift_r(v3, v4, b)));
-    } else {
-      // a chunk shared with the neighbouring tiles: its four words, whole
-      // where they lie inside [0, len), else byte by byte
-#pragma unroll
-      for (int wq = 0; wq < 4; wq++) {
-        const int64_t io = o + 4 * wq;
-        if (io >= 0 && io + 4 <= len) {
-          const uint32_t* iw = (const uint32_t*)img4;
-          const int ia = (int)io;
-          *(uint32_t*)(gp + 4 * wq) = __funnelshift_r(iw[ia >> 2], iw[(ia >> 2) + 1], (ia & 3) * 8);
-        } else if (io + 4 > 0 && io < len) {
-#pragma unroll
-          for (int bb = 0; bb < 4; bb++)
-            if (io + bb >= 0 && io + bb < len) gp[4 * wq + bb] = img[io + bb];
-        }
-      }
-    }
+  uint8_t* o = out + G;
+  const int s = (int)((0u - (uint32_t)(uintptr_t)o) & 15u);
+  const int nf = len >= s ? (len - s) >> 4 : 0;
+  uint4* dst = (uint4*)(o + s);
+  const int b = (s & 3) * 8;
+  switch (s >> 2) {
+    case 0: lane_copy_chunks<0>(img4, dst, nf, b, lane); break;
+    case 1: lane_copy_chunks<1>(img4, dst, nf, b, lane); break;
+    case 2: lane_copy_chunks<2>(img4, dst, nf, b, lane); break;
+    default: lane_copy_chunks<3>(img4, dst, nf, b, lane); break;
+  }
+  const int t0 = s + 16 * nf;  // first byte after the whole chunks
+  if (lane < 16) {
+    if (lane < s && lane < len) o[lane] = img[lane];
+    if (t0 + lane < len) o[t0 + lane] = img[t0 + lane];
   }
 }
 
@@ -1127,7 +1118,7 @@ __device__ __forceinline__ void lane_write(const lane::Plan& p, const uint4* slo
 }
 
 template <bool DELTA>
-__global__ void __launch_bounds__(kLThreads) pack_lane_kernel(PackArgs a) {
+__global__ void __launch_bounds__(kLThreads, 8) pack_lane_kernel(PackArgs a) {
   extern __shared__ uint4 smem4[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   LaneWarpSmem& W = ((LaneWarpSmem*)smem4)[warp];

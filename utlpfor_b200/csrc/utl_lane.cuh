@@ -362,22 +362,28 @@ __device__ void write_block(const Plan& p, const uint4* s4, uint8_t* o) {
 #pragma unroll
       for (int q = 0; q < 4; q++) put_bytes(xi + 4 * q, bm[q], 4);
     }
-    int rank = 0, dd = nc;
+    // exceptions in position order: the lowest set bit of the bitmap each time
+    uint32_t b0 = bm[0], b1 = bm[1], b2 = bm[2], b3 = bm[3];
+    int dd = nc, rank = 0;
     uint32_t ctrl = 0;
-    for (int q = 0; q < 4; q++) {
-      for (uint32_t mb = bm[q]; mb; mb &= mb - 1) {
-        const int pos = 32 * q + __ffs(mb) - 1;
-        const uint32_t hv = work_at<DELTA>(s, pos, p.base, p.zz) >> bw;  // bw < 32 with exceptions
-        const int l = svb_len_of(hv);
-        if (p.exc <= 16 && rank < 16) xi[rank] = (uint8_t)pos;
-        ctrl |= (uint32_t)(l - 1) << (2 * (rank & 3));
-        if (dd + l <= p.svb_len) put_bytes(svb + dd, hv, l);
-        dd += l;
-        if ((rank & 3) == 3 && (rank >> 2) < nc) {
-          svb[rank >> 2] = (uint8_t)ctrl;
-          ctrl = 0;
-        }
-        rank++;
+    for (; rank < p.exc; rank++) {
+      const int q = b0 ? 0 : b1 ? 1 : b2 ? 2 : 3;
+      const uint32_t wq = q == 0 ? b0 : q == 1 ? b1 : q == 2 ? b2 : b3;
+      const uint32_t rest = wq & (wq - 1);
+      b0 = q == 0 ? rest : b0;
+      b1 = q == 1 ? rest : b1;
+      b2 = q == 2 ? rest : b2;
+      b3 = q == 3 ? rest : b3;
+      const int pos = 32 * q + __ffs(wq) - 1;
+      const uint32_t hv = work_at<DELTA>(s, pos & 127, p.base, p.zz) >> bw;  // bw < 32 with exceptions
+      const int l = svb_len_of(hv);
+      if (p.exc <= 16) xi[rank] = (uint8_t)pos;
+      ctrl |= (uint32_t)(l - 1) << (2 * (rank & 3));
+      if (dd + l <= p.svb_len) put_bytes(svb + dd, hv, l);
+      dd += l;
+      if ((rank & 3) == 3) {
+        svb[rank >> 2] = (uint8_t)ctrl;
+        ctrl = 0;
       }
     }
     if ((rank & 3) && (rank >> 2) < nc) svb[rank >> 2] = (uint8_t)ctrl;
