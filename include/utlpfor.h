@@ -249,6 +249,20 @@ UTL_API int utl_unpack_streams_u64(const uint8_t *h_packed, size_t packed_len,
                            const uint64_t *h_val_off, int n_streams,
                            uint64_t *h_values);
 
+/* ==================== stream indexer ==================== */
+/* Block offsets of a packed stream that carries no index: the walk a
+ * caller does with BlockLength block after block from offset 0
+ * (block_length.go:8-65, caller pattern example_test.go:171-186), done on
+ * the device.  d_packed[0, packed_len) holds whole blocks back to back;
+ * d_block_off receives n_blocks + 1 offsets (capacity max_blocks + 1, the
+ * last entry is packed_len).  Synchronizes `stream`.  Returns UTL_OK, the
+ * BlockLength error of the first bad block (UTL_ERR_INVALID_BUFFER also
+ * when a block runs past the end) with *n_blocks = that block's index, or
+ * UTL_ERR_CAPACITY with *n_blocks = the block count. */
+UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
+                             uint64_t *d_block_off, int64_t max_blocks,
+                             int64_t *n_blocks, void *stream);
+
 /* ==================== tuning ==================== */
 /* Process-wide knobs of the batched kernels, set by the autotuner
  * (utlpfor_b200.tune); no counterpart in the reference.  Defaults are

@@ -169,3 +169,25 @@ def unpack_streams(packed, block_off, val_off, dtype=np.uint32, n_threads=4):
         err = L.utlo_unpack_streams_u32(_p(pk, C.c_uint8), _p(bo, C.c_uint64), _p(vo, C.c_uint64), len(vo) - 1,
                                         _p(out, C.c_uint32), n_threads)
     return out, err
+
+
+def index_stream(packed):
+    """The caller's BlockLength walk over a packed stream (block_length.go:
+    8-65, example_test.go:171-186): (offsets incl. the end, error code,
+    index of the bad block).  A block running past the end is
+    ErrInvalidBuffer, as the caller's Unpack of it would report."""
+    pk = np.ascontiguousarray(packed, dtype=np.uint8)
+    L = lib()
+    offs, pos = [], 0
+    n = C.c_size_t(0)
+    while pos < pk.size:
+        sub = pk[pos:]
+        err = L.utlo_block_length(_p(sub, C.c_uint8), sub.size, C.byref(n))
+        if err == 0 and pos + n.value > pk.size:
+            err = INVALID_BUFFER
+        if err != 0:
+            return offs, err, len(offs)
+        offs.append(pos)
+        pos += n.value
+    offs.append(pos)
+    return offs, OK, len(offs) - 1

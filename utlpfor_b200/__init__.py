@@ -248,5 +248,5 @@ def NewUint64():
     return Compressor64()
 
 
-from .batch import (BatchCodec, PackedBatch, get_batch, pack_batch, pack_streams, plan,  # noqa: E402
+from .batch import (BatchCodec, PackedBatch, get_batch, index_stream, pack_batch, pack_streams, plan,  # noqa: E402
                     unpack_batch, unpack_streams)

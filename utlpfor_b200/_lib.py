@@ -55,6 +55,7 @@ SIGNATURES = [
     ("utl_pack_streams_u64", C.c_int, [C.c_uint8, VP, PU64, C.c_int, VP, C.c_size_t, PU64, PU64, SZ]),
     ("utl_unpack_streams_u32", C.c_int, [VP, C.c_size_t, PU64, PU64, C.c_int, VP]),
     ("utl_unpack_streams_u64", C.c_int, [VP, C.c_size_t, PU64, PU64, C.c_int, VP]),
+    ("utl_index_stream", C.c_int, [VP, C.c_size_t, VP, C.c_int64, C.POINTER(C.c_int64), VP]),
     ("utl_set_knob", C.c_int, [C.c_int, C.c_int]),
     ("utl_get_knob", C.c_int, [C.c_int]),
     ("utl_launch_count", C.c_uint64, []),

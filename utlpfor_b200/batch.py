@@ -261,3 +261,30 @@ class BatchCodec:
 
     def error_bits(self):
         return int(self.err.item())
+
+
+def index_stream(packed, max_blocks=None):
+    """Block offsets of a packed stream without an index (a CUDA uint8
+    tensor of whole blocks back to back): the BlockLength walk of
+    block_length.go:8-65 done on the device.  Returns an int64 tensor of
+    n_blocks + 1 offsets (the last is the stream length); raises the
+    reference's error of the first bad block (its index in .block)."""
+    torch = _torch()
+    L = load()
+    nbytes = packed.numel()
+    cap = max_blocks if max_blocks is not None else nbytes // 64 + 16
+    while True:
+        out = torch.empty(cap + 1, dtype=torch.int64, device=packed.device)
+        n = C.c_int64(0)
+        rc = L.utl_index_stream(_ptr(packed), nbytes, _ptr(out), cap, C.byref(n), _stream())
+        if rc == 9 and max_blocks is None:  # capacity: n holds the block count
+            cap = n.value
+            continue
+        if rc != 0:
+            from . import _raise
+            try:
+                _raise(rc)
+            except Exception as e:
+                e.block = n.value
+                raise
+        return out[:n.value + 1]

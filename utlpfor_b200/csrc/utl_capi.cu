@@ -73,7 +73,7 @@ struct Ctx {
   uint8_t* d_stage = nullptr;  // device alias of h_stage
   uint8_t* d_tmp = nullptr;    // device copy of staged input
   // buffers of the host-buffer batch path
-  Grow values, val_off, bstart, packed, block_off, sbo, scratch, err;
+  Grow values, val_off, bstart, packed, block_off, sbo, scratch, err, index;
 
   int init() {
     UTL_CUDA(cudaGetDevice(&device));
@@ -88,7 +88,7 @@ struct Ctx {
     cudaGetDevice(&cur);
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
-    Grow* gs[] = {&values, &val_off, &bstart, &packed, &block_off, &sbo, &scratch, &err};
+    Grow* gs[] = {&values, &val_off, &bstart, &packed, &block_off, &sbo, &scratch, &err, &index};
     for (Grow* g : gs) g->release();
     if (d_tmp) cudaFree(d_tmp);
     if (h_stage) cudaFreeHost(h_stage);
@@ -650,6 +650,21 @@ int utl_unpack_streams_u32(const uint8_t* h_packed, size_t packed_len, const uin
 int utl_unpack_streams_u64(const uint8_t* h_packed, size_t packed_len, const uint64_t* h_block_off,
                            const uint64_t* h_val_off, int n_streams, uint64_t* h_values) {
   return unpack_streams(true, h_packed, packed_len, h_block_off, h_val_off, n_streams, h_values);
+}
+
+int utl_index_stream(const uint8_t* d_packed, size_t packed_len, uint64_t* d_block_off, int64_t max_blocks,
+                     int64_t* n_blocks, void* stream) {
+  if (!n_blocks || !d_block_off || max_blocks < 0 || (packed_len && !d_packed)) return UTL_ERR_ARG;
+  *n_blocks = 0;
+  Ctx* c = nullptr;
+  int rc = thread_ctx(&c);
+  if (rc != UTL_OK) return rc;
+  UTL_CUDA(c->index.ensure(launch::index_scratch_bytes(packed_len)));
+  cudaError_t ce = cudaSuccess;
+  rc = launch::index_stream(d_packed, packed_len, d_block_off, max_blocks, n_blocks, c->index.p, (cudaStream_t)stream,
+                            &ce);
+  if (rc < 0) return cuda_fail(ce);
+  return rc;
 }
 
 int utl_set_knob(int knob, int value) { return launch::set_knob(knob, value) == 0 ? UTL_OK : UTL_ERR_ARG; }

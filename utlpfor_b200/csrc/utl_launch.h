@@ -77,6 +77,9 @@ cudaError_t plain_unpack(bool u64, const uint8_t* src, int64_t staged, int64_t a
                          PlainResult* res, cudaStream_t st);
 cudaError_t plain_get(bool u64, int pos, const uint8_t* src, int64_t staged, int64_t avail, uint8_t* tmp,
                       PlainResult* res, cudaStream_t st);
+size_t index_scratch_bytes(uint64_t len);
+int index_stream(const uint8_t* p, uint64_t len, uint64_t* block_off, int64_t max_blocks, int64_t* n_blocks,
+                 void* scratch, cudaStream_t st, cudaError_t* cerr);
 int set_knob(int knob, int value);
 int get_knob(int knob);
 }  // namespace launch
