@@ -485,6 +485,7 @@ def main():
     ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-index", action="store_true", help="skip timing the stream indexer")
     ap.add_argument("--log2n", type=int, default=28, help="values per GPU of the c3 workloads (2^log2n)")
     ap.add_argument("--knob", action="append", default=[], help="kernel knob id=value (see utl_set_knob)")
     ap.add_argument("--serve-requests", type=int, default=10000, help="c5: requests per offered rate")
@@ -636,6 +637,28 @@ def main():
                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
                "timing": "host wall clock around synchronous C-ABI calls (pinned host buffers)"}
 
+    # the stream indexer over the packed result (outside the timed region):
+    # block offsets recovered from the bytes alone, checked against the pack's
+    index = None
+    if rank == 0 and not args.no_index:
+        pk_t = codec.packed[:packed_len]
+        bo_t = torch.empty(codec.n_blocks + 1, dtype=torch.int64, device=dev)
+        nbv = C.c_int64(0)
+        sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        rc = L.utl_index_stream(C.c_void_p(pk_t.data_ptr()), packed_len, C.c_void_p(bo_t.data_ptr()), codec.n_blocks,
+                                C.byref(nbv), sp)
+        assert rc == 0 and nbv.value == codec.n_blocks, (rc, nbv.value)
+        assert torch.equal(bo_t, codec.block_off), "indexer offsets differ from the pack's"
+        reps = 5
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            L.utl_index_stream(C.c_void_p(pk_t.data_ptr()), packed_len, C.c_void_p(bo_t.data_ptr()), codec.n_blocks,
+                               C.byref(nbv), sp)
+        ims = (time.perf_counter() - t0) / reps * 1e3
+        index = {"ms": ims, "packed_GBps": packed_len / (ims * 1e-3) / 1e9, "blocks": codec.n_blocks,
+                 "timing": "host wall clock around the synchronous call"}
+
     cpu = None
     if rank == 0 and not args.no_cpu and args.workload.startswith("c3"):
         threads = host_threads()
@@ -663,6 +686,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "index": index,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }

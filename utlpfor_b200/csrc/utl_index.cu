@@ -105,6 +105,29 @@ __device__ int64_t walk(const uint8_t* p, uint64_t len, int64_t pos, int64_t end
   return pos;
 }
 
+// Walk the chains from x (the stream's) and y (a partition's) forward, the
+// one behind each time, until they meet before `end`.  On a meeting
+// returns true with hx/hy = blocks each chain took to get there.
+__device__ bool meet(const uint8_t* p, uint64_t len, int64_t x, int64_t y, int64_t end, int64_t* hx, int64_t* hy) {
+  int64_t cx = 0, cy = 0;
+  while (x != y) {
+    if (x >= end || y >= end) return false;
+    uint64_t L;
+    if (x < y) {
+      if (block_length_at(p, len, (uint64_t)x, &L) != kOK) return false;
+      x += (int64_t)L;
+      cx++;
+    } else {
+      if (block_length_at(p, len, (uint64_t)y, &L) != kOK) return false;
+      y += (int64_t)L;
+      cy++;
+    }
+  }
+  *hx = cx;
+  *hy = cy;
+  return x < end;
+}
+
 __global__ void __launch_bounds__(kThreads) speculate_kernel(const uint8_t* p, uint64_t len, int64_t n_parts,
                                                              Part* parts) {
   const int64_t k = (int64_t)blockIdx.x * kThreads + threadIdx.x;
@@ -120,7 +143,9 @@ __global__ void __launch_bounds__(kThreads) speculate_kernel(const uint8_t* p, u
       int good = 0;
       for (; good < kSync && (uint64_t)q < len; good++) {
         uint64_t L;
-        if (block_length_at(p, len, (uint64_t)q, &L) != kOK) break;
+        // a start is accepted only on blocks a packer can emit (no block is
+        // longer than kMaxBlock); the walks keep BlockLength's own rules
+        if (block_length_at(p, len, (uint64_t)q, &L) != kOK || L > (uint64_t)kMaxBlock) break;
         q += (int64_t)L;
       }
       if (good == kSync || (uint64_t)q == len) entry = x;
@@ -162,14 +187,10 @@ __global__ void __launch_bounds__(kThreads) check_kernel(const uint8_t* p, uint6
         ok = true;
         tc = 0;
       } else if (y >= 0) {
-        const int64_t a = min(x, y), b = max(x, y);
-        int64_t c;
-        int err = 0;
-        int64_t epos;
-        const int64_t reach = walk(p, len, a, b, &c, &err, &epos);
-        if (reach == b) {
+        int64_t hx, hy;
+        if (meet(p, len, x, y, end, &hx, &hy)) {  // the chains share every block from the meeting on
           ok = true;
-          tc = x <= y ? r.count + c : r.count - c;
+          tc = hx + r.count - hy;
         }
       }
     }
@@ -219,11 +240,9 @@ __global__ void fixup_kernel(const uint8_t* p, uint64_t len, int64_t n_parts, Pa
       return;
     }
     if (q.entry >= 0 && q.exit >= 0) {
-      const int64_t a = min(e, q.entry), b = max(e, q.entry);
-      int64_t hops;
-      const int64_t reach = walk(p, len, a, b, &hops, &err, &epos);
-      if (reach == b) {
-        q.tcount = e <= q.entry ? q.count + hops : q.count - hops;
+      int64_t hx, hy;
+      if (meet(p, len, e, q.entry, nend, &hx, &hy)) {
+        q.tcount = hx + q.count - hy;
         q.ok = 1;
         return;
       }
