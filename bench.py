@@ -566,9 +566,8 @@ def main():
     unpack_ms = sum(b.elapsed_time(c) for _, b, c in ev) / args.steps
     step_ms = total_ms / args.steps
     if world > 1:
-        t = torch.tensor([step_ms, pack_ms, unpack_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms, pack_ms, unpack_ms = [float(x) for x in t.tolist()]
+        from utlpfor_b200.dist import max_over_ranks
+        step_ms, pack_ms, unpack_ms = max_over_ranks([step_ms, pack_ms, unpack_ms])
     assert torch.equal(out, values)
 
     value_bytes = n * esz
@@ -627,9 +626,8 @@ def main():
             e2e_step()
         e2e_s = (time.perf_counter() - t0) / e_steps
         if world > 1:
-            t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+            from utlpfor_b200.dist import max_over_ranks
+            e2e_s = max_over_ranks([e2e_s])[0]
         meta = 8 * (ns + 1)
         h2d = value_bytes + meta + packed_len + 8 * (nb + 1) + meta
         d2h = 8 * (nb + 1) + packed_len + value_bytes + 8
