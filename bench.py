@@ -516,12 +516,12 @@ def main():
     flag, is64 = wl["flag"], wl["is64"]
     esz = 8 if is64 else 4
     L = load()
-    for kv in args.knob:
-        k, v = kv.split("=")
-        assert L.utl_set_knob(int(k), int(v)) == 0, kv
     values, vo = make_workload(torch, args.workload, rank, dev, args.log2n)
     n = int(vo[-1])
-    codec = U.BatchCodec(vo, flag=flag, is64=is64, device=dev)
+    codec = U.BatchCodec(vo, flag=flag, is64=is64, device=dev)  # applies the tuned knobs of this GPU
+    for kv in args.knob:  # explicit knobs override them
+        k, v = kv.split("=")
+        assert L.utl_set_knob(int(k), int(v)) == 0, kv
     out = torch.empty_like(values)
 
     def barrier():

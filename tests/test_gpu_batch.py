@@ -27,7 +27,8 @@ def to_dev(torch, a):
 LENS = [1, 128, 300, 0, 257, 1000, 5, 129, 0, 4096, 77]
 
 
-@pytest.fixture(params=[0, 1], ids=["unpack_tiles", "unpack_pipelined"])
+@pytest.fixture(params=[0, 1, 2, 3], ids=["unpack_tiles", "unpack_pipelined", "unpack_pipelined_wide",
+                                          "unpack_pipelined_narrow"])
 def sched(request):
     from utlpfor_b200._lib import load
     L = load()

@@ -80,6 +80,40 @@ __device__ __forceinline__ void block_span(const uint64_t* val_off, const uint64
   *n = (int)min((uint64_t)kBlock, e - f);
 }
 
+// Stream of block b (largest s with block_start[s] <= b).
+__device__ __forceinline__ int stream_of(const uint64_t* bstart, int n_streams, int64_t b) {
+  int lo = 0, hi = n_streams;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if ((int64_t)bstart[mid] <= b) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+// The same, knowing the stream s0 of an earlier block: galloping from s0
+// (consecutive blocks are nearly always in the same or the next stream).
+__device__ __forceinline__ int stream_from(const uint64_t* bstart, int n_streams, int s0, int64_t b) {
+  int lo = s0, step = 1;
+  while (lo + step < n_streams && (int64_t)bstart[lo + step] <= b) {
+    lo += step;
+    step <<= 1;
+  }
+  int hi = min(n_streams, lo + step);
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if ((int64_t)bstart[mid] <= b) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+// First value index and value count of block b of stream s.
+__device__ __forceinline__ void span_in(const uint64_t* val_off, const uint64_t* bstart, int s, int64_t b,
+                                        uint64_t* first, int* n) {
+  const uint64_t f = val_off[s] + (uint64_t)(b - (int64_t)bstart[s]) * kBlock;
+  *first = f;
+  *n = (int)min((uint64_t)kBlock, val_off[s + 1] - f);
+}
+
 // Copy len bytes of a shared-memory slot (word aligned) to out[g..g+len):
 // whole 32-bit words where the global word lies inside the range, single
 // bytes at the two edges (those words are shared with neighbouring blocks).
@@ -571,9 +605,13 @@ __global__ void __launch_bounds__(kQThreads) unpack_quad_kernel(UnpackArgs a) {
 // chunks, no registers held) and the block offsets of the group after
 // that are loading.  Groups that do not fit a buffer take the one-block-
 // per-round path of unpack_quad_kernel.
-constexpr int kPStage = 8 * 264;  // per-buffer budget: 8 blocks of up to 264 bytes
+// per-buffer budget: 8 blocks of up to 264 bytes (narrow batches) or of up
+// to 528 bytes (batches whose blocks are wide)
+constexpr int kPStageNarrow = 8 * 264;
+constexpr int kPStageWide = 8 * 528;
+template <int STAGE>
 struct QuadPipeSmem {
-  uint4 stage[kQWarps][2][(kPStage + kQStagePad) / 16];
+  uint4 stage[kQWarps][2][(STAGE + kQStagePad) / 16];
   uint4 patch[kQWarps][8][kBlock / 4];
 };
 
@@ -611,6 +649,7 @@ struct GroupInfo {
   uint64_t off;   // lane l <= nb: block_off[b0 + l]
   int64_t b0;
   int nb;
+  int s0;         // stream of block b0 (lane 0; broadcast when used)
 };
 
 __device__ __forceinline__ GroupInfo group_load(const UnpackArgs& a, int64_t g, int lane) {
@@ -618,22 +657,36 @@ __device__ __forceinline__ GroupInfo group_load(const UnpackArgs& a, int64_t g, 
   gi.b0 = g * 8;
   gi.nb = gi.b0 < a.n_blocks ? (int)min((int64_t)8, a.n_blocks - gi.b0) : 0;
   gi.off = (gi.nb > 0 && lane <= gi.nb) ? a.block_off[gi.b0 + lane] : 0ull;
+  gi.s0 = (gi.nb > 0 && lane == 0) ? stream_of(a.block_start, a.n_streams, gi.b0) : 0;
   return gi;
 }
 
 // whether a group's contiguous bytes fit one staging buffer (warp-uniform)
+template <int STAGE>
 __device__ __forceinline__ bool group_fits(const UnpackArgs& a, const GroupInfo& gi, int lane) {
   const uint64_t next = __shfl_down_sync(kFull, gi.off, 1);
   const bool ok = lane >= gi.nb || (next >= gi.off && next - gi.off <= (uint64_t)kMaxBlock32 && next <= a.packed_len);
   const uint64_t o0 = __shfl_sync(kFull, gi.off, 0), o1 = __shfl_sync(kFull, gi.off, gi.nb);
   const int ph = (int)(((uintptr_t)a.packed + o0) & 15);
-  return __all_sync(kFull, ok) && (int64_t)(o1 - o0) + ph + 16 <= kPStage;
+  return __all_sync(kFull, ok) && (int64_t)(o1 - o0) + ph + 16 <= STAGE;
 }
 
+// Mean packed block length above which a batch takes the wide staging.
+constexpr uint64_t kWideMean = 240;
+
+// AUTO: the narrow and the wide instance are both launched; each works out
+// from the block offsets which of them the batch's mean block length calls
+// for, and the other returns at once (same inputs, same answer).
+template <int STAGE, bool AUTO>
 __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackArgs a) {
   extern __shared__ uint4 smem4[];
-  QuadPipeSmem& S = *(QuadPipeSmem*)smem4;
+  QuadPipeSmem<STAGE>& S = *(QuadPipeSmem<STAGE>*)smem4;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (AUTO) {
+    const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
+    const bool wide = span > kWideMean * (uint64_t)a.n_blocks;
+    if (wide != (STAGE == kPStageWide)) return;
+  }
   const int q = lane >> 2, j = lane & 3;
   const unsigned qm = quad::quad_mask(lane);
   const int64_t n_groups = (a.n_blocks + 7) / 8;
@@ -643,7 +696,7 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackAr
   uint32_t* patch = (uint32_t*)S.patch[warp][q];
 
   GroupInfo cur = group_load(a, g, lane);
-  bool cur_fits = group_fits(a, cur, lane);
+  bool cur_fits = group_fits<STAGE>(a, cur, lane);
   if (cur_fits)
     stage_bytes_async(S.stage[warp][0], a.packed, a.packed_len, __shfl_sync(kFull, cur.off, 0),
                       __shfl_sync(kFull, cur.off, cur.nb), lane);
@@ -652,7 +705,7 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackAr
   for (int it = 0; g < n_groups; it++, g += stride) {
     const int buf = it & 1;
     // put the next group in flight, and start loading the one after it
-    const bool nxt_fits = nxt.nb > 0 && group_fits(a, nxt, lane);
+    const bool nxt_fits = nxt.nb > 0 && group_fits<STAGE>(a, nxt, lane);
     if (nxt_fits)
       stage_bytes_async(S.stage[warp][buf ^ 1], a.packed, a.packed_len, __shfl_sync(kFull, nxt.off, 0),
                         __shfl_sync(kFull, nxt.off, nxt.nb), lane);
@@ -666,6 +719,7 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackAr
     const uint64_t s = __shfl_sync(kFull, cur.off, q), e = __shfl_sync(kFull, cur.off, q + 1);
     const bool bad = e < s || e - s > (uint64_t)kMaxBlock32 || e > a.packed_len;
     const int64_t b = cur.b0 + q;
+    const int s0 = __shfl_sync(kFull, cur.s0, 0);
     const int rounds = cur_fits ? 1 : nb;
     const uint4* stg = S.stage[warp][buf];
 #pragma unroll 1
@@ -681,7 +735,7 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackAr
       if (cur_fits ? q < nb : q == rd) {
         uint64_t first;
         int want;
-        block_span(a.val_off, a.block_start, a.n_streams, b, &first, &want);
+        span_in(a.val_off, a.block_start, stream_from(a.block_start, a.n_streams, s0, b), b, &first, &want);
         int status = kOK, ovf = 0;
         if (bad) {
           status = kErrCountMismatch;
@@ -928,7 +982,8 @@ __device__ __forceinline__ int lane_load_tile(const PackArgs& a, int64_t tile, u
   const int64_t gb = tile * 32 + lane;
   uint64_t first = 0;
   int n = 0;
-  if (gb < a.n_blocks) block_span(a.val_off, a.block_start, a.n_streams, gb, &first, &n);
+  const int s0 = __shfl_sync(kFull, lane == 0 ? stream_of(a.block_start, a.n_streams, tile * 32) : 0, 0);
+  if (gb < a.n_blocks) span_in(a.val_off, a.block_start, stream_from(a.block_start, a.n_streams, s0, gb), gb, &first, &n);
   const uint32_t* vals = (const uint32_t*)a.values;
   const uint64_t f0 = __shfl_sync(kFull, first, 0);
   const bool ok = n == kBlock && first == f0 + (uint64_t)kBlock * lane;
@@ -1522,6 +1577,30 @@ cudaError_t stream_offsets(const uint64_t* block_off, const uint64_t* bstart, in
 static int g_quad_pack_ctas = 0;
 static bool g_quad_unpack_cfg = false;
 static int g_pipe_ctas = 0;
+static int g_pipe_wide_ctas = 0;
+
+template <int STAGE, bool AUTO>
+static cudaError_t unpack_pipe(const UnpackArgs& a, cudaStream_t st, int& ctas) {
+  const size_t psmem = sizeof(QuadPipeSmem<STAGE>);
+  auto kern = unpack_quad_pipe_kernel<STAGE, AUTO>;
+  if (ctas == 0) {
+    for (const void* f : {(const void*)unpack_quad_pipe_kernel<STAGE, true>,
+                          (const void*)unpack_quad_pipe_kernel<STAGE, false>}) {
+      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
+      if (e != cudaSuccess) return e;
+      cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kern, kQThreads, psmem);
+    if (ctas <= 0) ctas = 1;
+  }
+  const int64_t groups = (a.n_blocks + 7) / 8;
+  int64_t grid = (int64_t)num_sms() * ctas;
+  const int64_t need = (groups + kQWarps - 1) / kQWarps;
+  if (grid > need) grid = need;
+  kern<<<(unsigned)grid, kQThreads, psmem, st>>>(a);
+  note_launch(1);
+  return cudaGetLastError();
+}
 // 0: one CTA per 32 blocks; 1: persistent pipelined warps (selectable for tuning)
 static int g_unpack_schedule = 1;
 static int g_pack_cap = 0;
@@ -1609,24 +1688,13 @@ cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
       g_quad_unpack_cfg = true;
     }
     if (a.n_blocks <= 0) return cudaSuccess;
-    if (g_unpack_schedule == 1) {
-      const size_t psmem = sizeof(QuadPipeSmem);
-      if (g_pipe_ctas == 0) {
-        cudaError_t e = cudaFuncSetAttribute(unpack_quad_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)psmem);
-        if (e != cudaSuccess) return e;
-        cudaFuncSetAttribute(unpack_quad_pipe_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_pipe_ctas, unpack_quad_pipe_kernel, kQThreads, psmem);
-        if (g_pipe_ctas <= 0) g_pipe_ctas = 1;
-      }
-      const int64_t groups = (a.n_blocks + 7) / 8;
-      int64_t grid = (int64_t)num_sms() * g_pipe_ctas;
-      const int64_t need = (groups + kQWarps - 1) / kQWarps;
-      if (grid > need) grid = need;
-      unpack_quad_pipe_kernel<<<(unsigned)grid, kQThreads, psmem, st>>>(a);
-      note_launch(1);
-      return cudaGetLastError();
+    if (g_unpack_schedule == 1) {  // by the batch's mean block length, decided on the device
+      cudaError_t e = unpack_pipe<kPStageNarrow, true>(a, st, g_pipe_ctas);
+      if (e != cudaSuccess) return e;
+      return unpack_pipe<kPStageWide, true>(a, st, g_pipe_wide_ctas);
     }
+    if (g_unpack_schedule == 2) return unpack_pipe<kPStageWide, false>(a, st, g_pipe_wide_ctas);
+    if (g_unpack_schedule == 3) return unpack_pipe<kPStageNarrow, false>(a, st, g_pipe_ctas);
     const int64_t grid = (a.n_blocks + kQTile - 1) / kQTile;
     unpack_quad_kernel<<<(unsigned)grid, kQThreads, smem, st>>>(a);
     note_launch(1);
@@ -1684,7 +1752,7 @@ cudaError_t plain_get(bool u64, int pos, const uint8_t* src, int64_t staged, int
 int set_knob(int knob, int value) {
   switch (knob) {
     case 0:  // UTL_KNOB_UNPACK_SCHEDULE
-      if (value != 0 && value != 1) return -1;
+      if (value < 0 || value > 3) return -1;
       g_unpack_schedule = value;
       return 0;
     case 1:  // UTL_KNOB_PACK_CTAS_PER_SM (0 = occupancy maximum)

@@ -4,7 +4,7 @@ Measures every candidate knob setting on a synthetic batch with the given
 shape on the current GPU and stores the fastest in
 utlpfor_b200/tuned/<gpu name>.json; apply() loads that file (if any) for
 the current GPU and sets the knobs.  Knobs (include/utlpfor.h):
-  0 UTL_KNOB_UNPACK_SCHEDULE   0 tiles, 1 persistent pipelined
+  0 UTL_KNOB_UNPACK_SCHEDULE   0 tiles, 1 persistent pipelined (staging by block size), 2/3 wide/narrow only
   1 UTL_KNOB_PACK_CTAS_PER_SM  0 occupancy maximum, else a cap
   2 UTL_KNOB_PACK_SCHEDULE     0 four threads per block, 1 one thread per block
 
