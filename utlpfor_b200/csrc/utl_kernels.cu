@@ -530,7 +530,7 @@ constexpr int kQImage = kQTile * 288;      // pack tile image budget
 
 struct QuadUnpackSmem {
   uint4 stage[kQWarps][(kQStage + kQStagePad) / 16];
-  uint4 patch[kQWarps][8][kBlock / 4];
+  uint4 patch[kQWarps][8][kBlock / 4 + 1];  // +16 B: quads start on different banks
 };
 
 __global__ void __launch_bounds__(kQThreads) unpack_quad_kernel(UnpackArgs a) {
@@ -579,9 +579,8 @@ __global__ void __launch_bounds__(kQThreads) unpack_quad_kernel(UnpackArgs a) {
     if (r.status == kOK && (r.count != want || r.consumed != len)) r.status = kErrCountMismatch;
     if (r.status == kOK) {
       uint32_t* op = (uint32_t*)a.values + first;
-      if (want == kBlock && ((uintptr_t)op & 15) == 0) {
-#pragma unroll
-        for (int v = 0; v < 8; v++) __stcs((uint4*)(op + 16 * v + 4 * j), make_uint4(x[v][0], x[v][1], x[v][2], x[v][3]));
+      if (want == kBlock) {
+        quad::quad_store_full(op, x, patch, j, qm);
       } else {
 #pragma unroll
         for (int v = 0; v < 8; v++)
@@ -612,7 +611,7 @@ constexpr int kPStageWide = 8 * 528;
 template <int STAGE>
 struct QuadPipeSmem {
   uint4 stage[kQWarps][2][(STAGE + kQStagePad) / 16];
-  uint4 patch[kQWarps][8][kBlock / 4];
+  uint4 patch[kQWarps][8][kBlock / 4 + 1];  // +16 B: quads start on different banks
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -751,10 +750,8 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackAr
           if (status == kOK && (r.count != want || r.consumed != len)) status = kErrCountMismatch;
           if (status == kOK) {
             uint32_t* op = (uint32_t*)a.values + first;
-            if (want == kBlock && ((uintptr_t)op & 15) == 0) {
-#pragma unroll
-              for (int v = 0; v < 8; v++)
-                __stcs((uint4*)(op + 16 * v + 4 * j), make_uint4(x[v][0], x[v][1], x[v][2], x[v][3]));
+            if (want == kBlock) {
+              quad::quad_store_full(op, x, patch, j, qm);
             } else {
 #pragma unroll
               for (int v = 0; v < 8; v++)

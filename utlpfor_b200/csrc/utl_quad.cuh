@@ -317,6 +317,37 @@ __device__ QResult quad_unpack_block(const Src& sb, int64_t blk, int64_t avail, 
 
 // ---------------------------------------------------------------- pack
 // Decisions of one uint32 block, phase A of the pack (scalar.go:126-235).
+// Store a full decoded block (quad layout: lane j holds words 16v+4j+k) at
+// op (4-byte aligned).  When op is 16-byte aligned each row is four 16-byte
+// stores.  Otherwise (m = op's word misalignment) the block goes through the
+// quad's 128-word shared buffer and lane j writes the aligned chunk that
+// starts at word 16v+4j+4-m; the first 4-m and last m words are stored
+// singly.
+__device__ __forceinline__ void quad_store_full(uint32_t* op, const uint32_t (&x)[8][4], uint32_t* buf, int j,
+                                                unsigned qm) {
+  const int m = (int)(((uintptr_t)op >> 2) & 3);
+  if (m == 0) {
+#pragma unroll
+    for (int v = 0; v < 8; v++) __stcs((uint4*)(op + 16 * v + 4 * j), make_uint4(x[v][0], x[v][1], x[v][2], x[v][3]));
+    return;
+  }
+  __syncwarp(qm);
+#pragma unroll
+  for (int v = 0; v < 8; v++) *(uint4*)(buf + 16 * v + 4 * j) = make_uint4(x[v][0], x[v][1], x[v][2], x[v][3]);
+  __syncwarp(qm);
+  const int sh = 4 - m;
+#pragma unroll
+  for (int v = 0; v < 8; v++) {
+    const int r = 16 * v + 4 * j + sh;
+    if (r + 4 <= kBlock) __stcs((uint4*)(op + r), make_uint4(buf[r], buf[r + 1], buf[r + 2], buf[r + 3]));
+  }
+  if (j == 0)
+    for (int k = 0; k < sh; k++) op[k] = buf[k];
+  if (j == 3)
+    for (int k = kBlock - m; k < kBlock; k++) op[k] = buf[k];
+  __syncwarp(qm);
+}
+
 struct QPlan {
   uint32_t header;
   uint32_t base;   // FOR base (u32 FOR)
