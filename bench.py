@@ -601,7 +601,7 @@ def main():
         h_out = torch.empty(n * esz, dtype=torch.uint8, pin_memory=True)
         h_packed = torch.empty(packed_len + 4096, dtype=torch.uint8, pin_memory=True)
         nb = codec.n_blocks
-        h_bo = np.zeros(nb + 1, dtype=np.uint64)
+        h_bo = torch.zeros(nb + 1, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
         h_vo = np.ascontiguousarray(vo, dtype=np.uint64)
         ns = len(vo) - 1
         olen = C.c_size_t(0)

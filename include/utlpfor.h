@@ -228,10 +228,13 @@ UTL_API int utl_get_batch_u64(const uint8_t *d_packed, size_t packed_len,
                       uint32_t *d_err, void *stream);
 
 /* ==================== batched (host buffers) ==================== */
-/* Same batches end to end from host memory: copies in, one batched pass,
- * copies out, on the calling thread's context.  Pinned host buffers give
- * full PCIe bandwidth.  *out_len receives the packed size; h_block_off
- * (n_blocks+1) and h_stream_byte_off (n_streams+1, optional) as above. */
+/* Same batches end to end from host memory: copies in, batched passes,
+ * copies out, on the calling thread's context.  Large batches run in
+ * pieces whose copies in, kernels and copies out overlap
+ * (UTL_KNOB_HOST_PIPELINE).  Pinned host buffers give full PCIe bandwidth
+ * and the overlap; pageable ones work at the speed of CUDA's staged copies.
+ * *out_len receives the packed size; h_block_off (n_blocks+1) and
+ * h_stream_byte_off (n_streams+1, optional) as above. */
 UTL_API int utl_pack_streams_u32(uint8_t flag, const uint32_t *h_values,
                          const uint64_t *h_val_off, int n_streams,
                          uint8_t *h_out, size_t out_cap, uint64_t *h_block_off,
@@ -275,10 +278,17 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *   UTL_KNOB_PACK_CTAS_PER_SM: cap on resident pack CTAs per SM (0 = the
  *     occupancy maximum).
  *   UTL_KNOB_PACK_SCHEDULE: uint32 pack kernel, 0 = four threads per block
- *     (CTA tiles), 1 = one thread per block (independent warp tiles). */
+ *     (CTA tiles), 1 = one thread per block (independent warp tiles).
+ *   UTL_KNOB_HOST_PIPELINE: the host-buffer batch calls, 0 = one pass
+ *     (all copies in, kernels, all copies out); 1 = batches of 64 MiB of
+ *     values or more are cut at block boundaries into pieces of
+ *     max(32 MiB, batch/16) whose copies in, kernels and copies out overlap
+ *     (the default); 2 = every batch in eighths (for tests).  Outputs are
+ *     the same in every mode. */
 #define UTL_KNOB_UNPACK_SCHEDULE 0
 #define UTL_KNOB_PACK_CTAS_PER_SM 1
 #define UTL_KNOB_PACK_SCHEDULE 2
+#define UTL_KNOB_HOST_PIPELINE 3
 UTL_API int utl_set_knob(int knob, int value);
 UTL_API int utl_get_knob(int knob);
 

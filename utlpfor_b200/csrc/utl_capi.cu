@@ -14,6 +14,7 @@
 #include <atomic>
 #include <mutex>
 #include <unordered_map>
+#include <vector>
 
 #include "../../include/utlpfor.h"
 #include "utl_launch.h"
@@ -66,6 +67,30 @@ struct Grow {
   }
 };
 
+// Pinned host memory that grows on demand.
+struct HostGrow {
+  uint8_t* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= cap) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max(n, (size_t)4096);
+    cudaError_t e = cudaHostAlloc((void**)&p, want, cudaHostAllocDefault);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+// Most pieces one host-buffer batch is cut into (one event pair each).
+constexpr int kMaxPieces = 32;
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -74,6 +99,12 @@ struct Ctx {
   uint8_t* d_tmp = nullptr;    // device copy of staged input
   // buffers of the host-buffer batch path
   Grow values, val_off, bstart, packed, block_off, sbo, scratch, err, index;
+  // the piecewise host-buffer pipeline: copies in on h2d, kernels on
+  // stream, copies out on d2h; ev_in[k] / ev_run[k] mark piece k's input
+  // resident / its kernels done
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t ev_in[kMaxPieces] = {}, ev_run[kMaxPieces] = {};
+  HostGrow h_meta;  // pinned landing area of the pack's block offsets
 
   int init() {
     UTL_CUDA(cudaGetDevice(&device));
@@ -83,16 +114,34 @@ struct Ctx {
     UTL_CUDA(cudaMalloc((void**)&d_tmp, kStageIn));
     return UTL_OK;
   }
+  int init_pipe() {
+    if (h2d) return UTL_OK;
+    for (int k = 0; k < kMaxPieces; k++) {
+      UTL_CUDA(cudaEventCreateWithFlags(&ev_in[k], cudaEventDisableTiming));
+      UTL_CUDA(cudaEventCreateWithFlags(&ev_run[k], cudaEventDisableTiming));
+    }
+    UTL_CUDA(cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking));
+    UTL_CUDA(cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking));
+    return UTL_OK;
+  }
   void destroy() {
     int cur = 0;
     cudaGetDevice(&cur);
     cudaSetDevice(device);
-    if (stream) cudaStreamSynchronize(stream);
+    cudaStream_t ss[] = {stream, h2d, d2h};
+    for (cudaStream_t s : ss)
+      if (s) cudaStreamSynchronize(s);
     Grow* gs[] = {&values, &val_off, &bstart, &packed, &block_off, &sbo, &scratch, &err, &index};
     for (Grow* g : gs) g->release();
+    h_meta.release();
+    for (int k = 0; k < kMaxPieces; k++) {
+      if (ev_in[k]) cudaEventDestroy(ev_in[k]);
+      if (ev_run[k]) cudaEventDestroy(ev_run[k]);
+    }
     if (d_tmp) cudaFree(d_tmp);
     if (h_stage) cudaFreeHost(h_stage);
-    if (stream) cudaStreamDestroy(stream);
+    for (cudaStream_t s : ss)
+      if (s) cudaStreamDestroy(s);
     cudaSetDevice(cur);
   }
   uint8_t* in_h() { return h_stage; }
@@ -530,6 +579,242 @@ static int first_error(uint32_t bits) {
   return UTL_OK;
 }
 
+// Host-buffer batches go through the piecewise pipeline when the knob
+// allows: 0 = never, 1 = batches of at least kPipeMinBytes of values, in
+// pieces of max(kPieceMinBytes, batch / 16), 2 = any batch, in eighths.
+static std::atomic<int> g_host_pipe{1};
+constexpr uint64_t kPipeMinBytes = 64ull << 20;
+constexpr uint64_t kPieceMinBytes = 32ull << 20;
+
+// A piece of a host-buffer batch: values [v0, v1) and blocks [b0, b1) of
+// the caller's arrays, as ns sub-streams whose value-offset table (ns + 1
+// entries, rebased to v0) starts at tab[t0].
+struct Piece {
+  uint64_t v0, v1;
+  int64_t b0, b1;
+  size_t t0;
+  int ns;
+};
+
+// Values per piece for a batch of nv values of esz bytes (0 = one piece).
+static uint64_t piece_target(uint64_t nv, size_t esz) {
+  const uint64_t B = UTL_BLOCK_SIZE;
+  const int mode = g_host_pipe.load(std::memory_order_relaxed);
+  uint64_t t = 0;
+  if (mode == 1 && nv * esz >= kPipeMinBytes) t = std::max(kPieceMinBytes, nv * esz / 16) / esz;
+  if (mode == 2) t = (nv + 7) / 8;
+  return t ? (t + B - 1) / B * B : 0;
+}
+
+// Cut the batch into pieces of about `target` values.  A piece ends at a
+// stream end or, inside a stream, at a multiple of 128 values from the
+// stream's start: every block's bytes depend on its own values only, so a
+// stream cut there packs to the same blocks and the pieces' outputs laid
+// end to end are the whole batch's.
+static void cut_pieces(const uint64_t* vo, int n_streams, uint64_t target, std::vector<Piece>& ps,
+                       std::vector<uint64_t>& tab) {
+  const uint64_t B = UTL_BLOCK_SIZE;
+  ps.clear();
+  tab.clear();
+  Piece p{vo[0], vo[0], 0, 0, 0, 0};
+  tab.push_back(0);
+  auto close = [&]() {
+    ps.push_back(p);
+    p = Piece{p.v1, p.v1, p.b1, p.b1, tab.size(), 0};
+    tab.push_back(0);
+  };
+  for (int s = 0; s < n_streams; s++) {
+    uint64_t left = vo[s + 1] - vo[s];
+    while (left) {
+      const uint64_t room = target - (p.v1 - p.v0);
+      uint64_t take = left;
+      if (take > room) {
+        take = room / B * B;
+        if (take == 0) {  // the piece holds more than target - 128 values
+          close();
+          continue;
+        }
+      }
+      left -= take;
+      p.v1 += take;
+      p.b1 += (int64_t)((take + B - 1) / B);
+      p.ns++;
+      tab.push_back(p.v1 - p.v0);
+      if (p.v1 - p.v0 == target) close();
+    }
+  }
+  if (p.ns) ps.push_back(p);
+  else tab.pop_back();
+}
+
+// Pack through the pipeline: piece k's values go in on h2d while piece
+// k-1 packs on the compute stream into its own worst-case region; when a
+// piece is done the host reads its packed size, places its block offsets
+// after the pieces before it and copies its bytes out on d2h, so the two
+// copy directions and the kernels overlap.
+static int pack_streams_piped(Ctx* c, bool u64, uint8_t flag, const void* h_values, const uint64_t* h_val_off,
+                              int n_streams, int64_t nb, const std::vector<Piece>& ps,
+                              const std::vector<uint64_t>& tab, uint8_t* h_out, size_t out_cap,
+                              uint64_t* h_block_off, uint64_t* h_sbo, size_t* out_len) {
+  const int P = (int)ps.size();
+  const size_t esz = u64 ? 8 : 4;
+  const uint64_t v0 = h_val_off[0], nv = h_val_off[n_streams] - v0;
+  const size_t maxb = (size_t)(u64 ? utl_max_block_length64(flag) : utl_max_block_length32(flag));
+  std::vector<size_t> reg(P + 1, 0);  // piece k packs into packed[reg[k], reg[k+1])
+  int64_t nb_max = 0;
+  for (int k = 0; k < P; k++) {
+    const int64_t n = ps[k].b1 - ps[k].b0;
+    nb_max = std::max(nb_max, n);
+    reg[k + 1] = reg[k] + (((size_t)n * maxb + 16 + 255) & ~(size_t)255);
+  }
+  int rc = c->init_pipe();
+  if (rc != UTL_OK) return rc;
+  UTL_CUDA(c->values.ensure(nv * esz));
+  UTL_CUDA(c->val_off.ensure(tab.size() * 8));
+  UTL_CUDA(c->bstart.ensure(tab.size() * 8));
+  UTL_CUDA(c->packed.ensure(reg[P]));
+  UTL_CUDA(c->block_off.ensure(((size_t)nb + P) * 8));  // piece k's nb_k + 1 offsets at b0 + k
+  UTL_CUDA(c->scratch.ensure(launch::pack_scratch_bytes(nb_max)));
+  UTL_CUDA(c->err.ensure(8));
+  UTL_CUDA(c->h_meta.ensure(((size_t)nb + P) * 8));
+  const cudaStream_t st = c->stream;
+  uint64_t* dtab = (uint64_t*)c->val_off.p;
+  uint64_t* dbs = (uint64_t*)c->bstart.p;
+  uint64_t* dbo = (uint64_t*)c->block_off.p;
+  const uint64_t* hbo = (const uint64_t*)c->h_meta.p;
+  UTL_CUDA(cudaMemsetAsync(c->err.p, 0, 4, st));
+  UTL_CUDA(cudaMemcpyAsync(dtab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, c->h2d));
+
+  int next = 0;        // first piece whose bytes are not yet placed
+  uint64_t base = 0;   // packed bytes of the pieces before it
+  // place pieces [next, upto) that are done (all of them when wait): only
+  // pieces already enqueued, since an event not yet recorded in this call
+  // still reports an earlier call's completion
+  auto place = [&](int upto, bool wait) -> int {
+    while (next < upto) {
+      cudaError_t e = wait ? cudaEventSynchronize(c->ev_run[next]) : cudaEventQuery(c->ev_run[next]);
+      if (e == cudaErrorNotReady) return UTL_OK;
+      if (e != cudaSuccess) return cuda_fail(e);
+      const Piece& q = ps[next];
+      const int64_t n = q.b1 - q.b0;
+      const uint64_t* rel = hbo + q.b0 + next;
+      for (int64_t i = 0; i < n; i++) h_block_off[q.b0 + i] = rel[i] + base;
+      const uint64_t len = rel[n];
+      if (len && h_out && base + len <= out_cap)
+        UTL_CUDA(cudaMemcpyAsync(h_out + base, (uint8_t*)c->packed.p + reg[next], len, cudaMemcpyDeviceToHost,
+                                 c->d2h));
+      base += len;
+      next++;
+    }
+    return UTL_OK;
+  };
+
+  for (int k = 0; k < P; k++) {
+    const Piece& q = ps[k];
+    const int64_t n = q.b1 - q.b0;
+    uint8_t* dv = (uint8_t*)c->values.p + (q.v0 - v0) * esz;
+    UTL_CUDA(cudaMemcpyAsync(dv, (const uint8_t*)h_values + q.v0 * esz, (q.v1 - q.v0) * esz, cudaMemcpyHostToDevice,
+                             c->h2d));
+    UTL_CUDA(cudaEventRecord(c->ev_in[k], c->h2d));
+    UTL_CUDA(cudaStreamWaitEvent(st, c->ev_in[k], 0));
+    cudaError_t e = launch::plan(dtab + q.t0, q.ns, dbs + q.t0, st);
+    if (e != cudaSuccess) return cuda_fail(e);
+    rc = pack_batch(u64, flag, dv, dtab + q.t0, dbs + q.t0, q.ns, n, (uint8_t*)c->packed.p + reg[k],
+                    reg[k + 1] - reg[k], dbo + q.b0 + k, nullptr, c->scratch.p, c->scratch.cap, (uint32_t*)c->err.p,
+                    st);
+    if (rc != UTL_OK) return rc;
+    UTL_CUDA(cudaMemcpyAsync(c->h_meta.p + (q.b0 + k) * 8, dbo + q.b0 + k, ((size_t)n + 1) * 8,
+                             cudaMemcpyDeviceToHost, st));
+    UTL_CUDA(cudaEventRecord(c->ev_run[k], st));
+    rc = place(k + 1, false);
+    if (rc != UTL_OK) return rc;
+  }
+  rc = place(P, true);
+  if (rc != UTL_OK) return rc;
+  uint32_t errbits = 0;
+  UTL_CUDA(cudaMemcpyAsync(&errbits, c->err.p, 4, cudaMemcpyDeviceToHost, st));
+  UTL_CUDA(cudaStreamSynchronize(st));
+  UTL_CUDA(cudaStreamSynchronize(c->d2h));
+  if (errbits) return first_error(errbits);
+  h_block_off[nb] = base;
+  if (h_sbo) {
+    int64_t b = 0;
+    for (int s = 0; s < n_streams; s++) {
+      h_sbo[s] = h_block_off[b];
+      b += (int64_t)((h_val_off[s + 1] - h_val_off[s] + UTL_BLOCK_SIZE - 1) / UTL_BLOCK_SIZE);
+    }
+    h_sbo[n_streams] = base;
+  }
+  *out_len = (size_t)base;
+  if (base > out_cap || (base && !h_out)) return UTL_ERR_CAPACITY;
+  return UTL_OK;
+}
+
+// Unpack through the pipeline: every piece's packed bytes and block
+// offsets are queued on h2d first; piece k unpacks once its bytes are in
+// and its values go out on d2h while later pieces still come in.  Piece k
+// reads bytes below round_up(block_off[b1], 16) when its offsets rise
+// monotonically, and all of them are in once its own copy is; a piece
+// whose offsets do not rise waits for the whole buffer, so its blocks
+// decode (or fail) exactly as in a single pass.
+static int unpack_streams_piped(Ctx* c, bool u64, const uint8_t* h_packed, size_t packed_len,
+                                const uint64_t* h_block_off, const uint64_t* h_val_off, int n_streams, int64_t nb,
+                                const std::vector<Piece>& ps, const std::vector<uint64_t>& tab, void* h_values) {
+  const int P = (int)ps.size();
+  const size_t esz = u64 ? 8 : 4;
+  const uint64_t v0 = h_val_off[0], nv = h_val_off[n_streams] - v0;
+  int rc = c->init_pipe();
+  if (rc != UTL_OK) return rc;
+  UTL_CUDA(c->values.ensure(nv * esz));
+  UTL_CUDA(c->val_off.ensure(tab.size() * 8));
+  UTL_CUDA(c->bstart.ensure(tab.size() * 8));
+  UTL_CUDA(c->packed.ensure(packed_len + 16));
+  UTL_CUDA(c->block_off.ensure(((size_t)nb + 1) * 8));
+  UTL_CUDA(c->err.ensure(8));
+  const cudaStream_t st = c->stream;
+  uint64_t* dtab = (uint64_t*)c->val_off.p;
+  uint64_t* dbs = (uint64_t*)c->bstart.p;
+  uint64_t* dbo = (uint64_t*)c->block_off.p;
+  uint8_t* dp = (uint8_t*)c->packed.p;
+  UTL_CUDA(cudaMemsetAsync(c->err.p, 0, 4, st));
+  UTL_CUDA(cudaMemcpyAsync(dtab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, c->h2d));
+  // piece k copies bytes [cut[k], cut[k+1]) of the packed buffer
+  std::vector<uint64_t> cut(P + 1, 0);
+  cut[P] = packed_len;
+  for (int k = 1; k < P; k++) {
+    const uint64_t o = std::min<uint64_t>(h_block_off[ps[k].b0], packed_len);
+    cut[k] = std::max(cut[k - 1], std::min<uint64_t>((o + 15) & ~(uint64_t)15, packed_len));
+  }
+  for (int k = 0; k < P; k++) {
+    const Piece& q = ps[k];
+    UTL_CUDA(cudaMemcpyAsync(dbo + q.b0, h_block_off + q.b0, ((size_t)(q.b1 - q.b0) + 1) * 8,
+                             cudaMemcpyHostToDevice, c->h2d));
+    if (cut[k + 1] > cut[k])
+      UTL_CUDA(cudaMemcpyAsync(dp + cut[k], h_packed + cut[k], cut[k + 1] - cut[k], cudaMemcpyHostToDevice, c->h2d));
+    UTL_CUDA(cudaEventRecord(c->ev_in[k], c->h2d));
+  }
+  for (int k = 0; k < P; k++) {
+    const Piece& q = ps[k];
+    bool rising = true;
+    for (int64_t b = q.b0; b < q.b1 && rising; b++) rising = h_block_off[b + 1] >= h_block_off[b];
+    UTL_CUDA(cudaStreamWaitEvent(st, c->ev_in[rising ? k : P - 1], 0));
+    cudaError_t e = launch::plan(dtab + q.t0, q.ns, dbs + q.t0, st);
+    if (e != cudaSuccess) return cuda_fail(e);
+    const size_t vb = (q.v0 - v0) * esz;
+    rc = unpack_batch(u64, dp, packed_len, dbo + q.b0, dtab + q.t0, dbs + q.t0, q.ns, q.b1 - q.b0,
+                      (uint8_t*)c->values.p + vb, nullptr, (uint32_t*)c->err.p, st);
+    if (rc != UTL_OK) return rc;
+    UTL_CUDA(cudaEventRecord(c->ev_run[k], st));
+    UTL_CUDA(cudaStreamWaitEvent(c->d2h, c->ev_run[k], 0));
+    UTL_CUDA(cudaMemcpyAsync((uint8_t*)h_values + q.v0 * esz, (uint8_t*)c->values.p + vb, (q.v1 - q.v0) * esz,
+                             cudaMemcpyDeviceToHost, c->d2h));
+  }
+  uint32_t errbits = 0;
+  UTL_CUDA(cudaMemcpyAsync(&errbits, c->err.p, 4, cudaMemcpyDeviceToHost, c->d2h));
+  UTL_CUDA(cudaStreamSynchronize(c->d2h));
+  return errbits ? first_error(errbits) : UTL_OK;
+}
+
 static int pack_streams(bool u64, uint8_t flag, const void* h_values, const uint64_t* h_val_off, int n_streams,
                         uint8_t* h_out, size_t out_cap, uint64_t* h_block_off, uint64_t* h_sbo, size_t* out_len) {
   if (!h_val_off || n_streams < 0 || !out_len || !h_block_off) return UTL_ERR_ARG;
@@ -540,6 +825,15 @@ static int pack_streams(bool u64, uint8_t flag, const void* h_values, const uint
   if (rc != UTL_OK) return rc;
   const size_t esz = u64 ? 8 : 4;
   const uint64_t v0 = h_val_off[0], nv = h_val_off[n_streams] - v0;
+  const uint64_t target = piece_target(nv, esz);
+  if (target && nv > target) {
+    std::vector<Piece> ps;
+    std::vector<uint64_t> tab;
+    cut_pieces(h_val_off, n_streams, target, ps, tab);
+    if (ps.size() >= 2 && ps.size() <= (size_t)kMaxPieces)
+      return pack_streams_piped(c, u64, flag, h_values, h_val_off, n_streams, nb, ps, tab, h_out, out_cap,
+                                h_block_off, h_sbo, out_len);
+  }
   const size_t maxb = (size_t)(u64 ? utl_max_block_length64(flag) : utl_max_block_length32(flag));
   UTL_CUDA(c->values.ensure(nv * esz));
   UTL_CUDA(c->val_off.ensure(((size_t)n_streams + 1) * 8));
@@ -598,6 +892,15 @@ static int unpack_streams(bool u64, const uint8_t* h_packed, size_t packed_len, 
   if (rc != UTL_OK) return rc;
   const size_t esz = u64 ? 8 : 4;
   const uint64_t v0 = h_val_off[0], nv = h_val_off[n_streams] - v0;
+  const uint64_t target = piece_target(nv, esz);
+  if (target && nv > target) {
+    std::vector<Piece> ps;
+    std::vector<uint64_t> tab;
+    cut_pieces(h_val_off, n_streams, target, ps, tab);
+    if (ps.size() >= 2 && ps.size() <= (size_t)kMaxPieces)
+      return unpack_streams_piped(c, u64, h_packed, packed_len, h_block_off, h_val_off, n_streams, nb, ps, tab,
+                                  h_values);
+  }
   UTL_CUDA(c->values.ensure(nv * esz));
   UTL_CUDA(c->val_off.ensure(((size_t)n_streams + 1) * 8));
   UTL_CUDA(c->bstart.ensure(((size_t)n_streams + 1) * 8));
@@ -667,8 +970,18 @@ int utl_index_stream(const uint8_t* d_packed, size_t packed_len, uint64_t* d_blo
   return rc;
 }
 
-int utl_set_knob(int knob, int value) { return launch::set_knob(knob, value) == 0 ? UTL_OK : UTL_ERR_ARG; }
-int utl_get_knob(int knob) { return launch::get_knob(knob); }
+int utl_set_knob(int knob, int value) {
+  if (knob == UTL_KNOB_HOST_PIPELINE) {
+    if (value < 0 || value > 2) return UTL_ERR_ARG;
+    g_host_pipe.store(value, std::memory_order_relaxed);
+    return UTL_OK;
+  }
+  return launch::set_knob(knob, value) == 0 ? UTL_OK : UTL_ERR_ARG;
+}
+int utl_get_knob(int knob) {
+  if (knob == UTL_KNOB_HOST_PIPELINE) return g_host_pipe.load(std::memory_order_relaxed);
+  return launch::get_knob(knob);
+}
 
 uint64_t utl_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 int utl_last_cuda_error(void) { return t_last_cuda; }
