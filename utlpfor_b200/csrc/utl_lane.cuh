@@ -307,6 +307,33 @@ __device__ __forceinline__ void pack_group(const uint32_t (&w)[8][4], uint32_t* 
   for (int i = 0; i < NW; i++) put_seg(pw, d4, sh, i, g, x[i]);
 }
 
+// Widths 8 and 16 take whole bytes of each value: a word is the low bytes
+// of four (two) consecutive rows, gathered with byte permutes.
+template <>
+__device__ __forceinline__ void pack_group<8>(const uint32_t (&w)[8][4], uint32_t* pw, int d4, int sh, int g) {
+  uint32_t x[2][4];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint32_t lo = __byte_perm(w[4 * i][k], w[4 * i + 1][k], 0x0040);
+      const uint32_t hi = __byte_perm(w[4 * i + 2][k], w[4 * i + 3][k], 0x0040);
+      x[i][k] = __byte_perm(lo, hi, 0x5410);
+    }
+  put_seg(pw, d4, sh, 0, g, x[0]);
+  put_seg(pw, d4, sh, 1, g, x[1]);
+}
+template <>
+__device__ __forceinline__ void pack_group<16>(const uint32_t (&w)[8][4], uint32_t* pw, int d4, int sh, int g) {
+  uint32_t x[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) x[i][k] = __byte_perm(w[2 * i][k], w[2 * i + 1][k], 0x5410);
+#pragma unroll
+  for (int i = 0; i < 4; i++) put_seg(pw, d4, sh, i, g, x[i]);
+}
+
 // Write the block at o (shared memory): header, StreamVByte length, FOR
 // base, the UTL payload (scalar.go:7-59: lane L's eight values packed LSB
 // first into bw/4 words, word w of lane L at byte 64w + 4L), then the
