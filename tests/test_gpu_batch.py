@@ -65,9 +65,9 @@ def test_pack_unpack_batch_u32(env, flag, kind, sched, psched):
     assert np.array_equal(out.cpu().numpy().view(np.uint32), vals)
 
 
-@pytest.mark.parametrize("flag", [0, 1, 2, 3, 4, 5])
-@pytest.mark.parametrize("kind", ["for64", "full", "walk", "fit32", "upper_for"])
-def test_pack_unpack_batch_u64(env, flag, kind):
+@pytest.mark.parametrize("flag", [0, 1, 2, 3, 4, 5, 6, 7, 8, 13])
+@pytest.mark.parametrize("kind", ["for64", "full", "walk", "fit32", "upper_for", "zero"])
+def test_pack_unpack_batch_u64(env, flag, kind, psched):
     U, torch = env
     rng = np.random.default_rng(500 + flag)
     vals, vo = streams(rng, LENS, kind, is64=True)
@@ -185,3 +185,29 @@ def test_large_round_trip_properties(env, sched, psched):
     assert hashlib.sha256(got.tobytes()).digest() == hashlib.sha256(want.tobytes()).digest()
     out = U.unpack_batch(pb)
     assert torch.equal(out, to_dev(torch, v))
+
+
+@pytest.mark.parametrize("flag", [0, 1])
+def test_large_u64_mix(env, flag, psched):
+    """2^21 uint64 values over 96 ragged streams mixing the three uint64
+    shapes (FOR64, two-block, delta walk): the pack is byte-identical to the
+    oracle under both pack schedules and the unpack restores every value."""
+    U, torch = env
+    rng = np.random.default_rng(64 + flag)
+    lens = rng.integers(1, 40000, 96)
+    lens[-1] = max(1, (1 << 21) - int(lens[:-1].sum())) if int(lens[:-1].sum()) < (1 << 21) else lens[-1]
+    kinds = ["for64", "full", "walk"]
+    vals, vo = [], [0]
+    for i, n in enumerate(lens):
+        v, _ = streams(rng, [int(n)], kinds[i % 3], is64=True)
+        vals.append(v)
+        vo.append(vo[-1] + int(n))
+    vals = np.concatenate(vals)
+    vo = np.array(vo, dtype=np.uint64)
+    want, wbo, _ = O.pack_streams(flag, vals, vo, n_threads=8)
+    pb = U.pack_batch(to_dev(torch, vals), vo, flag)
+    assert pb.packed_len == len(want)
+    assert np.array_equal(pb.packed[:pb.packed_len].cpu().numpy(), want)
+    assert np.array_equal(pb.block_off.cpu().numpy().view(np.uint64), wbo)
+    out = U.unpack_batch(pb)
+    assert torch.equal(out, to_dev(torch, vals))

@@ -960,11 +960,12 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
 // ------------------------------------------------------------------------
 constexpr int kLWarps = 1;
 constexpr int kLThreads = kLWarps * 32;
+template <bool U64>
 struct LaneWarpSmem {
   uint4 in[32 * lane::kSlot / 16];
-  uint4 img[lane::kImage / 16];
+  uint4 img[lane::Window<U64>::kImageBytes / 16];
 };
-static_assert(lane::kSlot % 16 == 0 && lane::kImage % 16 == 0, "16-byte slots");
+static_assert(lane::kSlot % 16 == 0 && lane::kImage % 16 == 0 && lane::kImage64 % 16 == 0, "16-byte slots");
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -1010,6 +1011,127 @@ __device__ __forceinline__ int lane_load_tile(const PackArgs& a, int64_t tile, u
   }
   cp_async_commit();
   return n;
+}
+
+// A tile of the uint64 lane pack is 16 uint64 blocks; block k's low words
+// go to slot 2k and its high words to slot 2k+1 (zero past the block's
+// count), so each slot holds one uint32 sub-block candidate.  The raw
+// block is first copied (cp.async, all blocks in flight at once) to the
+// start of its slot pair, then split in place: the warp holds a block in
+// registers between a read and a write separated by a barrier.  Returns
+// the value count of this lane's block (lane >> 1; 0 past the last block).
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ int lane_load_tile64(const PackArgs& a, int64_t tile, uint8_t* inb, int lane) {
+  const int64_t gb = tile * 16 + (lane & 15);
+  uint64_t first = 0;
+  int n = 0;
+  const int s0 = __shfl_sync(kFull, lane == 0 ? stream_of(a.block_start, a.n_streams, tile * 16) : 0, 0);
+  if (lane < 16 && gb < a.n_blocks)
+    span_in(a.val_off, a.block_start, stream_from(a.block_start, a.n_streams, s0, gb), gb, &first, &n);
+  const uint64_t* vals = (const uint64_t*)a.values;
+  constexpr int kPair = 2 * lane::kSlot;  // a block's slot pair; its raw 1 KB fits at the start
+  for (int k = 0; k < 16; k++) {
+    const uint64_t fk = __shfl_sync(kFull, first, k);
+    const int nk = __shfl_sync(kFull, n, k);
+    uint8_t* dst = inb + k * kPair;
+    const uint64_t* src = vals + fk;
+    if (nk == kBlock && ((uintptr_t)src & 15) == 0) {
+      cp_async16(dst + 16 * lane, src + 2 * lane);
+      cp_async16(dst + 16 * (lane + 32), src + 2 * (lane + 32));
+    } else {
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const int i = lane + 32 * r;
+        if (i < nk) cp_async8(dst + 8 * i, src + i);
+        else *(uint2*)(dst + 8 * i) = make_uint2(0u, 0u);
+      }
+    }
+  }
+  cp_async_commit();
+  cp_async_wait0();
+  __syncwarp();
+  // split: lane l's values 4l..4l+3 are raw bytes 32l..32l+31 of the pair
+  for (int k0 = 0; k0 < 16; k0 += 4) {
+    uint4 A[4], B[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint8_t* b = inb + (k0 + q) * kPair + 32 * lane;
+      A[q] = *(const uint4*)b;
+      B[q] = *(const uint4*)(b + 16);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      uint8_t* b = inb + (k0 + q) * kPair;
+      *(uint4*)(b + 16 * lane) = make_uint4(A[q].x, A[q].z, B[q].x, B[q].z);
+      *(uint4*)(b + lane::kSlot + 16 * lane) = make_uint4(A[q].y, A[q].w, B[q].y, B[q].w);
+    }
+  }
+  return __shfl_sync(kFull, n, lane >> 1);
+}
+
+// The shape of uint64 block lane >> 1 (packUint64Scalar, uint64.go:302-333),
+// worked out by the lane pair from the two slots, and this lane's sub-block:
+// FOR64 when !NoFOR && min > 0 && max - min < 2^32 (the low words become
+// x - min in place, packed with FOR off inside), else one block of the low
+// words when every value fits in 32 bits, else the low words (combine
+// bit, block2Len field) followed by the high words.  The pair splits the
+// 128 values; lane h reads its chunks rotated by h so the pair's 16-byte
+// reads fall in distinct banks.
+struct Shape64 {
+  int n;           // this lane's sub-block value count (0: none)
+  int mode;
+  uint32_t type_flags;
+  int flag;
+  uint64_t base64;
+  bool two;        // the block is written as two sub-blocks
+};
+__device__ __forceinline__ Shape64 lane_shape64(uint8_t* inb, int nk, int flag, int lane) {
+  const int t = lane >> 1, h = lane & 1;
+  uint32_t* lo = (uint32_t*)(inb + (2 * t) * lane::kSlot);
+  const uint32_t* hi = (const uint32_t*)(inb + (2 * t + 1) * lane::kSlot);
+  uint64_t mn = ~0ull, mx = 0ull;
+  uint32_t acc = 0;
+  for (int c = 0; c < 16; c++) {
+    const int i0 = 64 * h + 4 * ((c + h) & 15);
+    const uint4 L = *(const uint4*)(lo + i0), H = *(const uint4*)(hi + i0);
+    const uint32_t l4[4] = {L.x, L.y, L.z, L.w}, h4[4] = {H.x, H.y, H.z, H.w};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint64_t x = ((uint64_t)h4[q] << 32) | l4[q];
+      if (i0 + q < nk) {
+        mn = min(mn, x);
+        mx = max(mx, x);
+      }
+      acc |= h4[q];  // zero past the count
+    }
+  }
+  mn = min(mn, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)mn, 1));
+  mx = max(mx, (uint64_t)__shfl_xor_sync(kFull, (unsigned long long)mx, 1));
+  acc |= __shfl_xor_sync(kFull, acc, 1);
+  Shape64 sh;
+  const bool for64 = nk > 0 && !(flag & kNoFOR) && mn > 0 && (mx - mn) < (1ull << 32);
+  sh.two = nk > 0 && !for64 && acc != 0;
+  sh.n = (h == 0 || sh.two) ? nk : 0;
+  sh.mode = h ? kModePlain : (for64 ? kModeFor64 : (sh.two ? kModeCombine : kModePlain));
+  sh.type_flags = kTypeU64 | ((h == 0 && sh.two) ? kHdrCombine : 0u);
+  sh.flag = flag | (for64 ? kNoFOR : 0);
+  sh.base64 = for64 ? mn : 0;
+  if (for64) {
+    // the low 32 bits of x - min are the low word minus the low word of min
+    const uint32_t m32 = (uint32_t)mn;
+    for (int c = 0; c < 16; c++) {
+      const int i0 = 64 * h + 4 * ((c + h) & 15);
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (i0 + q < nk) lo[i0 + q] -= m32;
+    }
+  }
+  __syncwarp();
+  return sh;
 }
 
 // Tile offsets of the lane pack.  Every tile publishes its aggregate (its
@@ -1106,8 +1228,9 @@ __device__ __forceinline__ uint64_t lane_win_finish(const LaneScan& sc, LaneWin&
   return warp_sum_u64(sum);
 }
 
-// Take a tile, load it, plan its blocks and publish its aggregate.
-template <bool DELTA>
+// Take a tile, load it, plan its blocks and publish its aggregate.  U64:
+// lane pair 2k, 2k+1 holds uint64 block k as one or two sub-blocks.
+template <bool DELTA, bool U64>
 __device__ __forceinline__ void lane_take_and_plan(const PackArgs& a, const LaneScan& sc, uint8_t* inb, uint4* slot,
                                                    int lane, int64_t& t, int& n, lane::Plan& p, int& incl,
                                                    int& total) {
@@ -1115,12 +1238,26 @@ __device__ __forceinline__ void lane_take_and_plan(const PackArgs& a, const Lane
   if (lane == 0) tv = atomicAdd((unsigned long long*)a.counter, 1ull);
   t = (int64_t)__shfl_sync(kFull, tv, 0);
   if (t >= a.n_tiles) return;
-  n = lane_load_tile(a, t, inb, lane);
-  cp_async_wait0();
-  __syncwarp();
   p.len = 0;
   p.exc = 0;
-  if (n > 0) p = lane::plan_block<DELTA>(slot, n, a.flag);
+  if (U64) {
+    const int nk = lane_load_tile64(a, t, inb, lane);
+    __syncwarp();
+    const Shape64 sh = lane_shape64(inb, nk, a.flag, lane);
+    n = sh.n;
+    if (n > 0) {
+      p = lane::plan_block<DELTA>(slot, n, sh.flag, sh.type_flags, sh.mode);
+      p.base64 = sh.base64;
+    }
+    // block2Len of a combined pair: the upper-halves block's length
+    const int l_hi = __shfl_xor_sync(kFull, p.len, 1);
+    if (n > 0 && p.mode == kModeCombine) p.blk2 = l_hi;
+  } else {
+    n = lane_load_tile(a, t, inb, lane);
+    cp_async_wait0();
+    __syncwarp();
+    if (n > 0) p = lane::plan_block<DELTA>(slot, n, a.flag);
+  }
   incl = warp_incl_scan(p.len, lane);
   total = __shfl_sync(kFull, incl, 31);
   if (lane == 31) lane_publish(sc, t, (uint32_t)total);
@@ -1163,17 +1300,38 @@ __device__ __forceinline__ void lane_copy_out(const uint4* img4, int len, uint8_
   }
 }
 
+// block_off of the tile's blocks, once the tile's byte offset G is known
+// (a uint64 block's offset is its first sub-block's; its end, the pair's).
+template <bool U64>
+__device__ __forceinline__ void lane_block_offsets(const PackArgs& a, int64_t tile, int lane, int n, int off,
+                                                   int incl, uint64_t G) {
+  if (U64) {
+    const int pair_end = __shfl_xor_sync(kFull, incl, 1);
+    const int64_t gb = tile * 16 + (lane >> 1);
+    if (!(lane & 1) && n > 0) {
+      a.block_off[gb] = G + (uint64_t)off;
+      if (gb == a.n_blocks - 1) a.block_off[a.n_blocks] = G + (uint64_t)pair_end;
+    }
+  } else {
+    const int64_t gb = tile * 32 + lane;
+    if (n > 0) {
+      a.block_off[gb] = G + (uint64_t)off;
+      if (gb == a.n_blocks - 1) a.block_off[a.n_blocks] = G + (uint64_t)incl;
+    }
+  }
+}
+
 template <bool DELTA>
 __device__ __forceinline__ void lane_write(const lane::Plan& p, const uint4* slot, uint8_t* o) {
   if (__any_sync(__activemask(), p.exc > 0)) lane::write_block<DELTA, true>(p, slot, o);
   else lane::write_block<DELTA, false>(p, slot, o);
 }
 
-template <bool DELTA>
+template <bool DELTA, bool U64>
 __global__ void __launch_bounds__(kLThreads, 8) pack_lane_kernel(PackArgs a) {
   extern __shared__ uint4 smem4[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  LaneWarpSmem& W = ((LaneWarpSmem*)smem4)[warp];
+  LaneWarpSmem<U64>& W = ((LaneWarpSmem<U64>*)smem4)[warp];
   uint8_t* inb = (uint8_t*)W.in;
   uint8_t* img = (uint8_t*)W.img;
   uint4* slot = (uint4*)(inb + lane * lane::kSlot);
@@ -1200,7 +1358,7 @@ __global__ void __launch_bounds__(kLThreads, 8) pack_lane_kernel(PackArgs a) {
         const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
         const bool fits = G + (uint64_t)total <= a.out_cap;
         if (!fits && lane == 0 && a.err) atomicOr(a.err, 1u << 9);
-        const int my_round = n > 0 ? off / lane::kWindow : -1;
+        const int my_round = n > 0 ? off / lane::Window<U64>::kBytes : -1;
         for (int r = 0; r < n_rounds; r++) {
           const unsigned in_r = __ballot_sync(kFull, my_round == r);
           const unsigned in_next = __ballot_sync(kFull, my_round == r + 1);
@@ -1211,11 +1369,7 @@ __global__ void __launch_bounds__(kLThreads, 8) pack_lane_kernel(PackArgs a) {
           if (fits) lane_copy_out(W.img, end - base, a.out, G + (uint64_t)base, lane);
           __syncwarp();
         }
-        const int64_t gb = cur * 32 + lane;
-        if (n > 0) {
-          a.block_off[gb] = G + (uint64_t)off;
-          if (gb == a.n_blocks - 1) a.block_off[a.n_blocks] = G + (uint64_t)incl;
-        }
+        lane_block_offsets<U64>(a, cur, lane, n, off, incl, G);
         prev = cur;
         prev_incl = G + (uint64_t)total;
       }
@@ -1225,25 +1379,22 @@ __global__ void __launch_bounds__(kLThreads, 8) pack_lane_kernel(PackArgs a) {
     // published while the current tile's window loads are in flight
     const int64_t done = cur;
     const int d_n = n, d_off = off, d_incl = incl, d_total = total, d_rounds = n_rounds;
-    lane_take_and_plan<DELTA>(a, sc, inb, slot, lane, cur, n, p, incl, total);
+    lane_take_and_plan<DELTA, U64>(a, sc, inb, slot, lane, cur, n, p, incl, total);
     if (done >= 0 && d_rounds <= 1) {
       const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
       if (G + (uint64_t)d_total <= a.out_cap) lane_copy_out(W.img, d_total, a.out, G, lane);
       else if (lane == 0 && a.err) atomicOr(a.err, 1u << 9);
-      const int64_t gb = done * 32 + lane;
-      if (d_n > 0) {
-        a.block_off[gb] = G + (uint64_t)d_off;
-        if (gb == a.n_blocks - 1) a.block_off[a.n_blocks] = G + (uint64_t)d_incl;
-      }
+      lane_block_offsets<U64>(a, done, lane, d_n, d_off, d_incl, G);
       prev = done;
       prev_incl = G + (uint64_t)d_total;
       __syncwarp();
     }
     if (cur >= a.n_tiles) break;
-    // blocks are a prefix of the lanes; their start offsets pick the rounds
+    // the last lane with a block (a prefix of the lanes, or every even lane
+    // and some odd ones for uint64) and the start offsets pick the rounds
     const unsigned act = __ballot_sync(kFull, n > 0);
     const int last = act ? 31 - __clz(act) : 0;
-    n_rounds = act ? __shfl_sync(kFull, incl - p.len, last) / lane::kWindow + 1 : 0;
+    n_rounds = act ? __shfl_sync(kFull, incl - p.len, last) / lane::Window<U64>::kBytes + 1 : 0;
   }
 }
 
@@ -1603,34 +1754,47 @@ static int g_unpack_schedule = 1;
 static int g_pack_cap = 0;
 
 static int g_pack_schedule = 1;
-static int g_lane_pack_ctas = 0;
+static int g_lane_pack_ctas = 0, g_lane_pack64_ctas = 0;
 
-static cudaError_t pack_lane(const PackArgs& a_in, cudaStream_t st) {
+static cudaError_t pack_lane(const PackArgs& a_in, cudaStream_t st, bool u64) {
   PackArgs a = a_in;
-  a.n_tiles = (a.n_blocks + 31) / 32;
-  const size_t smem = sizeof(LaneWarpSmem) * kLWarps;
+  a.n_tiles = u64 ? (a.n_blocks + 15) / 16 : (a.n_blocks + 31) / 32;
+  const size_t smem = (u64 ? sizeof(LaneWarpSmem<true>) : sizeof(LaneWarpSmem<false>)) * kLWarps;
   if (g_lane_pack_ctas == 0) {
-    for (int d = 0; d < 2; d++) {
-      const void* f = d ? (const void*)pack_lane_kernel<true> : (const void*)pack_lane_kernel<false>;
-      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const void* fs[4] = {(const void*)pack_lane_kernel<false, false>, (const void*)pack_lane_kernel<true, false>,
+                         (const void*)pack_lane_kernel<false, true>, (const void*)pack_lane_kernel<true, true>};
+    for (int i = 0; i < 4; i++) {
+      const size_t sm = (i >= 2 ? sizeof(LaneWarpSmem<true>) : sizeof(LaneWarpSmem<false>)) * kLWarps;
+      cudaError_t e = cudaFuncSetAttribute(fs[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       if (e != cudaSuccess) return e;
-      cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+      cudaFuncSetAttribute(fs[i], cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_lane_pack_ctas, pack_lane_kernel<false>, kLThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_lane_pack_ctas, pack_lane_kernel<false, false>, kLThreads,
+                                                  sizeof(LaneWarpSmem<false>) * kLWarps);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_lane_pack64_ctas, pack_lane_kernel<false, true>, kLThreads,
+                                                  sizeof(LaneWarpSmem<true>) * kLWarps);
     if (g_lane_pack_ctas <= 0) g_lane_pack_ctas = 1;
+    if (g_lane_pack64_ctas <= 0) g_lane_pack64_ctas = 1;
   }
-  const int per_sm = (g_pack_cap > 0 && g_pack_cap < g_lane_pack_ctas) ? g_pack_cap : g_lane_pack_ctas;
+  const int occ = u64 ? g_lane_pack64_ctas : g_lane_pack_ctas;
+  const int per_sm = (g_pack_cap > 0 && g_pack_cap < occ) ? g_pack_cap : occ;
   int64_t grid = (int64_t)num_sms() * per_sm;
   if (grid * kLWarps > a.n_tiles) grid = (a.n_tiles + kLWarps - 1) / kLWarps;
   if (grid < 1) grid = 1;
-  if (a.flag & kDelta) pack_lane_kernel<true><<<(unsigned)grid, kLThreads, smem, st>>>(a);
-  else pack_lane_kernel<false><<<(unsigned)grid, kLThreads, smem, st>>>(a);
+  const bool d = (a.flag & kDelta) != 0;
+  if (u64) {
+    if (d) pack_lane_kernel<true, true><<<(unsigned)grid, kLThreads, smem, st>>>(a);
+    else pack_lane_kernel<false, true><<<(unsigned)grid, kLThreads, smem, st>>>(a);
+  } else {
+    if (d) pack_lane_kernel<true, false><<<(unsigned)grid, kLThreads, smem, st>>>(a);
+    else pack_lane_kernel<false, false><<<(unsigned)grid, kLThreads, smem, st>>>(a);
+  }
   note_launch(1);
   return cudaGetLastError();
 }
 
 cudaError_t pack(bool u64, const PackArgs& a_in, cudaStream_t st) {
-  if (!u64 && g_pack_schedule == 1) return pack_lane(a_in, st);
+  if (g_pack_schedule == 1) return pack_lane(a_in, st, u64);
   if (!u64) {
     PackArgs a = a_in;
     a.n_tiles = (a.n_blocks + kQTile - 1) / kQTile;

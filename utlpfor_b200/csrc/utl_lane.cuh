@@ -1,4 +1,5 @@
-// utl_lane.cuh -- thread-per-block UTL-PFOR pack of uint32 blocks.
+// utl_lane.cuh -- thread-per-block UTL-PFOR pack of uint32 blocks (and of
+// the uint32 sub-blocks a uint64 block is written as).
 //
 // One thread owns one 128-value block end to end.  The block's values sit
 // in a 528-byte shared-memory slot (natural order: value i at word i, so
@@ -19,12 +20,24 @@ namespace utl {
 namespace lane {
 
 constexpr int kSlot = 528;        // one block's 512 value bytes + a 16-byte bank stagger
-constexpr int kMaxLen = 520;      // largest u32 block the pack emits: header + 512 payload + 4 FOR
+// Largest block the pack emits: header + 512 payload bytes + a FOR base (a
+// uint64 sub-block: the 8-byte FOR64 base, or a FOR base and the 2-byte
+// block2Len field), rounded up.
+constexpr int kMaxLen = 528;
 // A tile's image holds the blocks that start in a window of kWindow bytes
 // (a tile whose blocks are larger is written and copied out in rounds),
 // plus the last block's overhang and the slack the copy-out reads.
 constexpr int kWindow = 7168;
 constexpr int kImage = (kWindow + kMaxLen + 32 + 15) / 16 * 16;
+// The uint64 pack's tiles run to 32 sub-blocks of up to 528 bytes (two-block
+// shapes): a wider window keeps them to fewer rounds, at one warp less per SM.
+constexpr int kWindow64 = 10240;
+constexpr int kImage64 = (kWindow64 + kMaxLen + 32 + 15) / 16 * 16;
+template <bool U64>
+struct Window {
+  static constexpr int kBytes = U64 ? kWindow64 : kWindow;
+  static constexpr int kImageBytes = U64 ? kImage64 : kImage;
+};
 
 // 4-bit bucket counter of a value: bucket b = clz/4 (zero values drop out).
 __device__ __forceinline__ uint32_t nib(uint32_t x) { return quad::shl_clamp(1u, (uint32_t)__clz(x) & ~3u); }
@@ -67,9 +80,12 @@ __device__ __forceinline__ int svb_data_bytes(uint32_t E, uint32_t O, int bw) {
 struct Plan {
   uint32_t header;
   uint32_t base;  // FOR base, 0 without FOR
+  uint64_t base64;  // FOR64 base (mode kModeFor64)
+  int mode;       // kModePlain, or a uint64 sub-block shape (kModeCombine, kModeFor64)
+  int blk2;       // kModeCombine: the upper-halves block's length (block2Len)
   int bw;
   int exc;
-  int forb;       // FOR base bytes (0/1/2/4)
+  int forb;       // FOR base bytes (0/1/2/4; 8 for the FOR64 base)
   int p_off;      // payload offset in the block
   int idx_sz;
   int svb_len;    // StreamVByte bytes (control + data)
@@ -178,8 +194,11 @@ __device__ __forceinline__ void raw_stats(const uint4* s4, uint32_t& mn, uint32_
 // The block's decisions and length (PackUint32: for.go:95-126 FOR,
 // delta.go:23-48 delta/zigzag, select_bitwidth.go:20-72 width and
 // exceptions, exceptions.go:138-186 exception index, svb.go StreamVByte).
+// type_flags and mode describe uint64 sub-blocks (uint64.go:124-182): the
+// header's integer type and combine bit, and the FOR64 base or block2Len
+// field in front of the payload.
 template <bool DELTA>
-__device__ Plan plan_block(uint4* s4, int n, int flag) {
+__device__ Plan plan_block(uint4* s4, int n, int flag, uint32_t type_flags = kTypeU32, int mode = kModePlain) {
   uint32_t* s = (uint32_t*)s4;
   const bool need_mm = !(flag & kNoFOR);
   const bool need_raw_hist = !(flag & kNoFOR) || !DELTA;
@@ -191,7 +210,7 @@ __device__ Plan plan_block(uint4* s4, int n, int flag) {
     mn = 0xFFFFFFFFu;
     for (int i = 0; i < n; i++) mn = min(mn, s[i]);
   }
-  uint32_t hflags = kTypeU32 | ((uint32_t)(flag & kSpecial) << 14);
+  uint32_t hflags = type_flags | ((uint32_t)(flag & kSpecial) << 14);
   bool use_for = false;
   uint32_t base = 0;
   int fw = 0;
@@ -240,8 +259,12 @@ __device__ Plan plan_block(uint4* s4, int n, int flag) {
   p.exc = exc;
   p.base = base;
   p.zz = zz;
-  p.forb = use_for ? ((1 << fw) >> 1) : 0;
-  p.p_off = 4 + (exc ? 2 : 0) + p.forb;
+  p.base64 = 0;
+  p.mode = mode;
+  p.blk2 = 0;
+  p.forb = mode == kModeFor64 ? 8 : (use_for ? ((1 << fw) >> 1) : 0);
+  if (mode == kModeFor64) hflags |= 3u << 15;
+  p.p_off = 4 + (exc ? 2 : 0) + p.forb + (mode == kModeCombine ? 2 : 0);
   p.header = (uint32_t)(n & 0xFF) | ((uint32_t)(bw >> 2) << 8) | hflags | ((uint32_t)exc << 24);
   p.idx_sz = exc == 0 ? 0 : (exc <= 16 ? exc : 16);
   p.svb_len = exc ? ((exc + 3) >> 2) + svb_data_bytes(E, O, bw) : 0;
@@ -346,7 +369,13 @@ __device__ void write_block(const Plan& p, const uint4* s4, uint8_t* o) {
     put_bytes(o + 4, (uint32_t)p.svb_len, 2);
     m = 6;
   }
-  if (p.forb) put_bytes(o + m, p.base, p.forb);
+  if (p.mode == kModeFor64) {
+    put_bytes(o + m, (uint32_t)p.base64, 4);
+    put_bytes(o + m + 4, (uint32_t)(p.base64 >> 32), 4);
+  } else if (p.forb) {
+    put_bytes(o + m, p.base, p.forb);
+  }
+  if (p.mode == kModeCombine) put_bytes(o + m + p.forb, (uint32_t)p.blk2, 2);
   const int bw = p.bw;
   uint8_t* pay = o + p.p_off;
   const uint32_t mask = bw >= 32 ? 0xFFFFFFFFu : ((1u << bw) - 1u);  // exceptions are above it
