@@ -152,6 +152,40 @@ def test_unpack_batch_corrupt_blocks(env, sched):
             assert np.array_equal(outv[128 * b:128 * b + 128], ov)
 
 
+@pytest.mark.parametrize("flag", [0, 1])
+def test_unpack_batch_corrupt_blocks_u64(env, sched, flag):
+    """uint64 blocks (two-block and FOR64 shapes) with a damaged byte fail
+    their own status with the reference's error class; the others decode."""
+    U, torch = env
+    rng = np.random.default_rng(7 + flag)
+    parts, vo = [], [0]
+    for kind in ("full", "for64", "walk"):
+        v, _ = streams(rng, [128 * 20], kind, is64=True)
+        parts.append(v)
+        vo.append(vo[-1] + len(v))
+    vals = np.concatenate(parts)
+    vo = np.array(vo, dtype=np.uint64)
+    packed, bo, _ = O.pack_streams(flag, vals, vo)
+    bad = packed.copy()
+    victims = [2, 11, 19, 23, 35, 44, 58]
+    for b in victims:
+        bad[int(bo[b]) + int(rng.integers(0, int(bo[b + 1] - bo[b])))] ^= 0x5A
+    pb = U.pack_batch(to_dev(torch, vals), vo, flag)
+    dev_bad = torch.from_numpy(bad).cuda()
+    status = torch.zeros(pb.n_blocks, dtype=torch.int32, device="cuda")
+    out = U.unpack_batch(pb, block_status=status, check=False, packed=dev_bad)
+    st = status.cpu().numpy()
+    outv = out.cpu().numpy().view(np.uint64)
+    for b in range(pb.n_blocks):
+        blk = bad[int(bo[b]):int(bo[b + 1])]
+        ov, oc, oerr, oovf = O.unpack_u64(blk)
+        if oerr == 0 and (len(ov) != 128 or oc != len(blk)):
+            oerr = 8
+        assert (st[b] & 0xFF, st[b] >> 8) == (oerr, oovf), b
+        if oerr == 0:
+            assert np.array_equal(outv[128 * b:128 * b + 128], ov)
+
+
 def test_host_buffer_streams(env):
     U, torch = env
     rng = np.random.default_rng(12)
