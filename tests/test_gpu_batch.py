@@ -245,3 +245,22 @@ def test_large_u64_mix(env, flag, psched):
     assert np.array_equal(pb.block_off.cpu().numpy().view(np.uint64), wbo)
     out = U.unpack_batch(pb)
     assert torch.equal(out, to_dev(torch, vals))
+
+
+@pytest.mark.parametrize("flag", [0, 1, 2, 6])
+@pytest.mark.parametrize("kind", ["exc", "sorted", "walk"])
+def test_misaligned_whole_tiles(env, flag, kind, psched):
+    """Long streams that start 1, 2 or 3 values past a 16-byte boundary, so
+    whole tiles of 32 blocks load misaligned; the last tile ends at the end
+    of the values.  Bytes and offsets equal the oracle's."""
+    U, torch = env
+    rng = np.random.default_rng(900 + flag)
+    lens = [5, 128 * 100, 3, 128 * 70 + 17, 1, 128 * 64, 2, 128 * 33 + 1, 128 * 65]
+    vals, vo = streams(rng, lens, kind)
+    want, wbo, wso = O.pack_streams(flag, vals, vo)
+    pb = U.pack_batch(to_dev(torch, vals), vo, flag)
+    assert pb.packed_len == len(want)
+    assert np.array_equal(pb.packed[:pb.packed_len].cpu().numpy(), want)
+    assert np.array_equal(pb.block_off.cpu().numpy().view(np.uint64), wbo)
+    out = U.unpack_batch(pb)
+    assert torch.equal(out, to_dev(torch, vals))

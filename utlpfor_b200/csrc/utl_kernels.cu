@@ -976,20 +976,40 @@ __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_g
 // Issue the loads of tile `tile` into the slots; returns this lane's block
 // value count (0 past the last block).  Whole, contiguous, 16-byte aligned
 // tiles go through cp.async; others are loaded and zero-padded per block.
-__device__ __forceinline__ int lane_load_tile(const PackArgs& a, int64_t tile, uint8_t* inb, int lane) {
+// The 33 aligned chunks per slot of a misaligned contiguous tile (out of
+// line: the aligned tiles' loop stays small).
+__device__ __noinline__ void lane_issue_shifted(uint8_t* inb, const uint8_t* src, int lane) {
+  for (int c = lane; c < 32 * 33; c += 32) {
+    const int k = c / 33, q = c - 33 * k;
+    cp_async16(inb + k * lane::kSlot + 16 * q, src + 512 * k + 16 * q);
+  }
+}
+
+__device__ __forceinline__ int lane_load_tile(const PackArgs& a, int64_t tile, uint8_t* inb, int lane, int& shift) {
   const int64_t gb = tile * 32 + lane;
   uint64_t first = 0;
   int n = 0;
+  shift = 0;
   const int s0 = __shfl_sync(kFull, lane == 0 ? stream_of(a.block_start, a.n_streams, tile * 32) : 0, 0);
   if (gb < a.n_blocks) span_in(a.val_off, a.block_start, stream_from(a.block_start, a.n_streams, s0, gb), gb, &first, &n);
   const uint32_t* vals = (const uint32_t*)a.values;
   const uint64_t f0 = __shfl_sync(kFull, first, 0);
-  const bool ok = n == kBlock && first == f0 + (uint64_t)kBlock * lane;
-  if (__all_sync(kFull, ok) && (((uintptr_t)(vals + f0)) & 15) == 0) {
+  const bool whole = __all_sync(kFull, n == kBlock && first == f0 + (uint64_t)kBlock * lane);
+  const int mis = (int)(((uintptr_t)(vals + f0) >> 2) & 3);  // words past a 16-byte boundary
+  if (whole && mis == 0) {
     const uint8_t* src = (const uint8_t*)(vals + f0) + 16 * lane;
     uint8_t* dst = inb + 16 * lane;
 #pragma unroll 8
     for (int k = 0; k < 32; k++) cp_async16(dst + k * lane::kSlot, src + 512 * k);
+  } else if (whole && (((uintptr_t)vals) & 15) == 0 && f0 - (uint64_t)mis >= a.val_off[0] &&
+             f0 - (uint64_t)mis + 32 * kBlock + 4 <= a.val_off[a.n_streams]) {
+    // one contiguous run that starts mis words into a 16-byte chunk: each
+    // slot takes the 33 aligned chunks that cover its block (the 33rd fills
+    // the bank stagger) and is shifted down by mis words once loaded
+    // (lane_realign_slot).  The chunks stay inside the values the stream
+    // table describes.
+    lane_issue_shifted(inb, (const uint8_t*)(vals + f0 - mis), lane);
+    shift = mis;
   } else {
     // block by block: whole 16-byte aligned blocks in 16-byte copies, the
     // others value by value; positions past the block's count are zeroed
@@ -1011,6 +1031,24 @@ __device__ __forceinline__ int lane_load_tile(const PackArgs& a, int64_t tile, u
   }
   cp_async_commit();
   return n;
+}
+
+// Shift a slot loaded mis (1..3) words late down to word 0: chunk c takes
+// words mis..mis+3 of chunks c and c+1 (in place, ascending; 33 chunks in).
+template <int M>
+__device__ __forceinline__ void realign_chunks(uint4* s4) {
+  uint4 a = s4[0];
+  for (int c = 0; c < 32; c++) {
+    const uint4 b = s4[c + 1];
+    const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    s4[c] = make_uint4(w[M], w[M + 1], w[M + 2], w[M + 3]);
+    a = b;
+  }
+}
+__device__ __noinline__ void lane_realign_slot(uint4* slot, int shift) {
+  if (shift == 1) realign_chunks<1>(slot);
+  else if (shift == 2) realign_chunks<2>(slot);
+  else if (shift == 3) realign_chunks<3>(slot);
 }
 
 // A tile of the uint64 lane pack is 16 uint64 blocks; block k's low words
@@ -1253,9 +1291,11 @@ __device__ __forceinline__ void lane_take_and_plan(const PackArgs& a, const Lane
     const int l_hi = __shfl_xor_sync(kFull, p.len, 1);
     if (n > 0 && p.mode == kModeCombine) p.blk2 = l_hi;
   } else {
-    n = lane_load_tile(a, t, inb, lane);
+    int shift;
+    n = lane_load_tile(a, t, inb, lane, shift);
     cp_async_wait0();
     __syncwarp();
+    if (shift) lane_realign_slot(slot, shift);  // warp-uniform; each lane its own slot
     if (n > 0) p = lane::plan_block<DELTA>(slot, n, a.flag);
   }
   incl = warp_incl_scan(p.len, lane);
