@@ -18,8 +18,12 @@
 
 #include "../../include/utlpfor.h"
 #include "utl_launch.h"
+#include "utl_pieces.h"
 
 namespace utl {
+
+using pieces::Piece;
+using pieces::cut_pieces;
 
 static std::atomic<uint64_t> g_launches{0};
 void note_launch(int n) { g_launches.fetch_add((uint64_t)n, std::memory_order_relaxed); }
@@ -586,16 +590,6 @@ static std::atomic<int> g_host_pipe{1};
 constexpr uint64_t kPipeMinBytes = 64ull << 20;
 constexpr uint64_t kPieceMinBytes = 32ull << 20;
 
-// A piece of a host-buffer batch: values [v0, v1) and blocks [b0, b1) of
-// the caller's arrays, as ns sub-streams whose value-offset table (ns + 1
-// entries, rebased to v0) starts at tab[t0].
-struct Piece {
-  uint64_t v0, v1;
-  int64_t b0, b1;
-  size_t t0;
-  int ns;
-};
-
 // Values per piece for a batch of nv values of esz bytes (0 = one piece).
 static uint64_t piece_target(uint64_t nv, size_t esz) {
   const uint64_t B = UTL_BLOCK_SIZE;
@@ -606,46 +600,6 @@ static uint64_t piece_target(uint64_t nv, size_t esz) {
   return t ? (t + B - 1) / B * B : 0;
 }
 
-// Cut the batch into pieces of about `target` values.  A piece ends at a
-// stream end or, inside a stream, at a multiple of 128 values from the
-// stream's start: every block's bytes depend on its own values only, so a
-// stream cut there packs to the same blocks and the pieces' outputs laid
-// end to end are the whole batch's.
-static void cut_pieces(const uint64_t* vo, int n_streams, uint64_t target, std::vector<Piece>& ps,
-                       std::vector<uint64_t>& tab) {
-  const uint64_t B = UTL_BLOCK_SIZE;
-  ps.clear();
-  tab.clear();
-  Piece p{vo[0], vo[0], 0, 0, 0, 0};
-  tab.push_back(0);
-  auto close = [&]() {
-    ps.push_back(p);
-    p = Piece{p.v1, p.v1, p.b1, p.b1, tab.size(), 0};
-    tab.push_back(0);
-  };
-  for (int s = 0; s < n_streams; s++) {
-    uint64_t left = vo[s + 1] - vo[s];
-    while (left) {
-      const uint64_t room = target - (p.v1 - p.v0);
-      uint64_t take = left;
-      if (take > room) {
-        take = room / B * B;
-        if (take == 0) {  // the piece holds more than target - 128 values
-          close();
-          continue;
-        }
-      }
-      left -= take;
-      p.v1 += take;
-      p.b1 += (int64_t)((take + B - 1) / B);
-      p.ns++;
-      tab.push_back(p.v1 - p.v0);
-      if (p.v1 - p.v0 == target) close();
-    }
-  }
-  if (p.ns) ps.push_back(p);
-  else tab.pop_back();
-}
 
 // Pack through the pipeline: piece k's values go in on h2d while piece
 // k-1 packs on the compute stream into its own worst-case region; when a
