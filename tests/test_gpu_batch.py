@@ -221,7 +221,7 @@ def test_large_round_trip_properties(env, sched, psched):
     assert torch.equal(out, to_dev(torch, v))
 
 
-@pytest.mark.parametrize("flag", [0, 1])
+@pytest.mark.parametrize("flag", [0, 1, 3, 4])
 def test_large_u64_mix(env, flag, psched):
     """2^21 uint64 values over 96 ragged streams mixing the three uint64
     shapes (FOR64, two-block, delta walk): the pack is byte-identical to the
