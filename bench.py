@@ -14,7 +14,8 @@ Printed: ONE JSON line (rank 0).  value = uncompressed round-trip
 throughput (bytes of values packed + bytes of values unpacked) / step
 time, summed over ranks.  e2e = the same metric through the host-buffer
 C-ABI calls (utl_pack_streams_u32 / utl_unpack_streams_u32) with pinned
-host memory, copies included.
+host memory, copies included.  get = 2^20 random GetUint32 queries over the
+packed result in one batched launch (queries/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                     [--workload c3|c3-nofor|c3-nopatch|c1|c2|c4|c5]
@@ -486,6 +487,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-index", action="store_true", help="skip timing the stream indexer")
+    ap.add_argument("--no-get", action="store_true", help="skip timing the batched Get")
     ap.add_argument("--log2n", type=int, default=28, help="values per GPU of the c3 workloads (2^log2n)")
     ap.add_argument("--knob", action="append", default=[], help="kernel knob id=value (see utl_set_knob)")
     ap.add_argument("--serve-requests", type=int, default=10000, help="c5: requests per offered rate")
@@ -657,6 +659,38 @@ def main():
         index = {"ms": ims, "packed_GBps": packed_len / (ims * 1e-3) / 1e9, "blocks": codec.n_blocks,
                  "timing": "host wall clock around the synchronous call"}
 
+    # GetUint32 / GetUint64 over the packed result: 2^20 queries, a stream
+    # drawn uniformly among the non-empty ones and a position uniformly in
+    # it, one batched launch; checked against the values, timed with CUDA
+    # events (reported as queries/s: a query reads a few bytes of a block)
+    get = None
+    if rank == 0 and not args.no_get:
+        nq = 1 << 20
+        gq = torch.Generator(device=dev)
+        gq.manual_seed(4321)
+        starts_t = torch.from_numpy(vo[:-1].astype(np.int64)).to(dev)
+        lens_t = torch.from_numpy((vo[1:] - vo[:-1]).astype(np.int64)).to(dev)
+        live = torch.nonzero(lens_t > 0).flatten()
+        q_s = live[torch.randint(0, live.numel(), (nq,), device=dev, generator=gq)]
+        q_p = (torch.rand(nq, device=dev, generator=gq, dtype=torch.float64) * lens_t[q_s].double()).long()
+        q_p = torch.minimum(q_p, lens_t[q_s] - 1)
+        q_stream = q_s.to(torch.int32)
+        q_out = torch.empty(nq, dtype=values.dtype, device=dev)
+        codec.get(q_stream, q_p, q_out)
+        assert torch.equal(q_out, values[starts_t[q_s] + q_p]), "Get results differ from the values"
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 10
+        torch.cuda.synchronize()
+        g0.record()
+        for _ in range(reps):
+            codec.get(q_stream, q_p, q_out)
+        g1.record()
+        torch.cuda.synchronize()
+        gms = g0.elapsed_time(g1) / reps
+        get = {"queries": nq, "ms": gms, "queries_per_s": nq / (gms * 1e-3),
+               "queries_drawn": "stream uniform among non-empty streams, position uniform in it",
+               "timing": "CUDA events, one batched launch per call"}
+
     cpu = None
     if rank == 0 and not args.no_cpu and args.workload.startswith("c3"):
         threads = host_threads()
@@ -685,6 +719,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": e2e,
             "index": index,
+            "get": get,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
