@@ -264,3 +264,33 @@ def test_misaligned_whole_tiles(env, flag, kind, psched):
     assert np.array_equal(pb.block_off.cpu().numpy().view(np.uint64), wbo)
     out = U.unpack_batch(pb)
     assert torch.equal(out, to_dev(torch, vals))
+
+
+def test_pack_window_shapes(env):
+    """The uint32 lane pack picks its image window from the previous pack's
+    block density.  Small blocks twice (the second pack takes the small
+    window), then large blocks right after (the small window with many
+    rounds), then again (the large window): every output equals the
+    oracle's."""
+    U, torch = env
+    from utlpfor_b200._lib import load
+    L = load()
+    old = L.utl_get_knob(2)
+    assert L.utl_set_knob(2, 1) == 0
+    try:
+        rng = np.random.default_rng(55)
+        n = 1 << 18
+        small = rng.integers(0, 2**8, n, dtype=np.uint64)
+        m = rng.random(n) < 0.02
+        small[m] = rng.integers(2**8, 2**32, int(m.sum()), dtype=np.uint64)
+        small = small.astype(np.uint32)
+        large = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+        vo = np.array([0, n], dtype=np.uint64)
+        for vals, flag in ((small, 0), (small, 0), (large, 4), (large, 4), (small, 0)):
+            want, wbo, _ = O.pack_streams(flag, vals, vo, n_threads=8)
+            pb = U.pack_batch(to_dev(torch, vals), vo, flag)
+            assert pb.packed_len == len(want)
+            assert np.array_equal(pb.packed[:pb.packed_len].cpu().numpy(), want)
+            assert np.array_equal(pb.block_off.cpu().numpy().view(np.uint64), wbo)
+    finally:
+        L.utl_set_knob(2, old)

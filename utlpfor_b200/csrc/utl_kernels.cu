@@ -960,12 +960,12 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
 // ------------------------------------------------------------------------
 constexpr int kLWarps = 1;
 constexpr int kLThreads = kLWarps * 32;
-template <bool U64>
+template <int SHAPE>
 struct LaneWarpSmem {
   uint4 in[32 * lane::kSlot / 16];
-  uint4 img[lane::Window<U64>::kImageBytes / 16];
+  uint4 img[lane::Window<SHAPE>::kImageBytes / 16];
 };
-static_assert(lane::kSlot % 16 == 0 && lane::kImage % 16 == 0 && lane::kImage64 % 16 == 0, "16-byte slots");
+static_assert(lane::kSlot % 16 == 0, "16-byte slots");
 
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -1356,7 +1356,13 @@ __device__ __forceinline__ void lane_block_offsets(const PackArgs& a, int64_t ti
     const int64_t gb = tile * 32 + lane;
     if (n > 0) {
       a.block_off[gb] = G + (uint64_t)off;
-      if (gb == a.n_blocks - 1) a.block_off[a.n_blocks] = G + (uint64_t)incl;
+      if (gb == a.n_blocks - 1) {
+        a.block_off[a.n_blocks] = G + (uint64_t)incl;
+        if (a.stats) {  // the batch's packed bytes and blocks, for the next launch's shape
+          a.stats[0] = G + (uint64_t)incl;
+          a.stats[1] = (uint64_t)a.n_blocks;
+        }
+      }
     }
   }
 }
@@ -1367,11 +1373,12 @@ __device__ __forceinline__ void lane_write(const lane::Plan& p, const uint4* slo
   else lane::write_block<DELTA, false>(p, slot, o);
 }
 
-template <bool DELTA, bool U64>
+template <bool DELTA, int SHAPE>
 __global__ void __launch_bounds__(kLThreads, 8) pack_lane_kernel(PackArgs a) {
+  constexpr bool U64 = SHAPE == 2;
   extern __shared__ uint4 smem4[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  LaneWarpSmem<U64>& W = ((LaneWarpSmem<U64>*)smem4)[warp];
+  LaneWarpSmem<SHAPE>& W = ((LaneWarpSmem<SHAPE>*)smem4)[warp];
   uint8_t* inb = (uint8_t*)W.in;
   uint8_t* img = (uint8_t*)W.img;
   uint4* slot = (uint4*)(inb + lane * lane::kSlot);
@@ -1398,7 +1405,7 @@ __global__ void __launch_bounds__(kLThreads, 8) pack_lane_kernel(PackArgs a) {
         const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
         const bool fits = G + (uint64_t)total <= a.out_cap;
         if (!fits && lane == 0 && a.err) atomicOr(a.err, 1u << 9);
-        const int my_round = n > 0 ? off / lane::Window<U64>::kBytes : -1;
+        const int my_round = n > 0 ? off / lane::Window<SHAPE>::kBytes : -1;
         for (int r = 0; r < n_rounds; r++) {
           const unsigned in_r = __ballot_sync(kFull, my_round == r);
           const unsigned in_next = __ballot_sync(kFull, my_round == r + 1);
@@ -1434,7 +1441,7 @@ __global__ void __launch_bounds__(kLThreads, 8) pack_lane_kernel(PackArgs a) {
     // and some odd ones for uint64) and the start offsets pick the rounds
     const unsigned act = __ballot_sync(kFull, n > 0);
     const int last = act ? 31 - __clz(act) : 0;
-    n_rounds = act ? __shfl_sync(kFull, incl - p.len, last) / lane::Window<U64>::kBytes + 1 : 0;
+    n_rounds = act ? __shfl_sync(kFull, incl - p.len, last) / lane::Window<SHAPE>::kBytes + 1 : 0;
   }
 }
 
@@ -1794,40 +1801,64 @@ static int g_unpack_schedule = 1;
 static int g_pack_cap = 0;
 
 static int g_pack_schedule = 1;
-static int g_lane_pack_ctas = 0, g_lane_pack64_ctas = 0;
+static int g_lane_ctas[3] = {0, 0, 0};  // resident CTAs per SM of each window shape
+// Mapped pinned words the uint32 lane pack's last block fills with the
+// batch's packed bytes and block count; the next launch reads them (without
+// waiting) to pick its window shape.  Only a performance hint: a stale or
+// torn pair picks the other shape, whose output is the same.
+static uint64_t* g_lane_stats = nullptr;
+static uint64_t* g_lane_stats_dev = nullptr;
+
+template <bool DELTA, int SHAPE>
+static void launch_lane(const PackArgs& a, int64_t grid, cudaStream_t st) {
+  pack_lane_kernel<DELTA, SHAPE><<<(unsigned)grid, kLThreads, sizeof(LaneWarpSmem<SHAPE>) * kLWarps, st>>>(a);
+}
 
 static cudaError_t pack_lane(const PackArgs& a_in, cudaStream_t st, bool u64) {
   PackArgs a = a_in;
   a.n_tiles = u64 ? (a.n_blocks + 15) / 16 : (a.n_blocks + 31) / 32;
-  const size_t smem = (u64 ? sizeof(LaneWarpSmem<true>) : sizeof(LaneWarpSmem<false>)) * kLWarps;
-  if (g_lane_pack_ctas == 0) {
-    const void* fs[4] = {(const void*)pack_lane_kernel<false, false>, (const void*)pack_lane_kernel<true, false>,
-                         (const void*)pack_lane_kernel<false, true>, (const void*)pack_lane_kernel<true, true>};
-    for (int i = 0; i < 4; i++) {
-      const size_t sm = (i >= 2 ? sizeof(LaneWarpSmem<true>) : sizeof(LaneWarpSmem<false>)) * kLWarps;
-      cudaError_t e = cudaFuncSetAttribute(fs[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (g_lane_ctas[0] == 0) {
+    const void* fs[6] = {(const void*)pack_lane_kernel<false, 0>, (const void*)pack_lane_kernel<true, 0>,
+                         (const void*)pack_lane_kernel<false, 1>, (const void*)pack_lane_kernel<true, 1>,
+                         (const void*)pack_lane_kernel<false, 2>, (const void*)pack_lane_kernel<true, 2>};
+    const size_t sms[3] = {sizeof(LaneWarpSmem<0>) * kLWarps, sizeof(LaneWarpSmem<1>) * kLWarps,
+                           sizeof(LaneWarpSmem<2>) * kLWarps};
+    for (int i = 0; i < 6; i++) {
+      cudaError_t e = cudaFuncSetAttribute(fs[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms[i / 2]);
       if (e != cudaSuccess) return e;
       cudaFuncSetAttribute(fs[i], cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_lane_pack_ctas, pack_lane_kernel<false, false>, kLThreads,
-                                                  sizeof(LaneWarpSmem<false>) * kLWarps);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_lane_pack64_ctas, pack_lane_kernel<false, true>, kLThreads,
-                                                  sizeof(LaneWarpSmem<true>) * kLWarps);
-    if (g_lane_pack_ctas <= 0) g_lane_pack_ctas = 1;
-    if (g_lane_pack64_ctas <= 0) g_lane_pack64_ctas = 1;
+    for (int sh = 0; sh < 3; sh++) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_lane_ctas[sh], fs[2 * sh], kLThreads, sms[sh]);
+      if (g_lane_ctas[sh] <= 0) g_lane_ctas[sh] = 1;
+    }
+    if (cudaHostAlloc((void**)&g_lane_stats, 2 * sizeof(uint64_t), cudaHostAllocMapped | cudaHostAllocPortable) ==
+        cudaSuccess) {
+      g_lane_stats[0] = g_lane_stats[1] = 0;
+      if (cudaHostGetDevicePointer((void**)&g_lane_stats_dev, g_lane_stats, 0) != cudaSuccess)
+        g_lane_stats_dev = nullptr;
+    } else {
+      g_lane_stats = nullptr;
+      cudaGetLastError();
+    }
   }
-  const int occ = u64 ? g_lane_pack64_ctas : g_lane_pack_ctas;
+  int shape = 2;
+  if (!u64) {
+    const volatile uint64_t* sv = g_lane_stats;
+    const uint64_t bytes = sv ? sv[0] : 0, blocks = sv ? sv[1] : 0;
+    shape = (blocks > 0 && bytes <= blocks * (uint64_t)lane::kSmallBlock) ? 1 : 0;
+    a.stats = g_lane_stats_dev;
+  }
+  const int occ = g_lane_ctas[shape];
   const int per_sm = (g_pack_cap > 0 && g_pack_cap < occ) ? g_pack_cap : occ;
   int64_t grid = (int64_t)num_sms() * per_sm;
   if (grid * kLWarps > a.n_tiles) grid = (a.n_tiles + kLWarps - 1) / kLWarps;
   if (grid < 1) grid = 1;
   const bool d = (a.flag & kDelta) != 0;
-  if (u64) {
-    if (d) pack_lane_kernel<true, true><<<(unsigned)grid, kLThreads, smem, st>>>(a);
-    else pack_lane_kernel<false, true><<<(unsigned)grid, kLThreads, smem, st>>>(a);
-  } else {
-    if (d) pack_lane_kernel<true, false><<<(unsigned)grid, kLThreads, smem, st>>>(a);
-    else pack_lane_kernel<false, false><<<(unsigned)grid, kLThreads, smem, st>>>(a);
+  switch (shape) {
+    case 0: d ? launch_lane<true, 0>(a, grid, st) : launch_lane<false, 0>(a, grid, st); break;
+    case 1: d ? launch_lane<true, 1>(a, grid, st) : launch_lane<false, 1>(a, grid, st); break;
+    default: d ? launch_lane<true, 2>(a, grid, st) : launch_lane<false, 2>(a, grid, st); break;
   }
   note_launch(1);
   return cudaGetLastError();

@@ -26,17 +26,22 @@ constexpr int kSlot = 528;        // one block's 512 value bytes + a 16-byte ban
 constexpr int kMaxLen = 528;
 // A tile's image holds the blocks that start in a window of kWindow bytes
 // (a tile whose blocks are larger is written and copied out in rounds),
-// plus the last block's overhang and the slack the copy-out reads.
+// plus the last block's overhang and the slack the copy-out reads.  The
+// window trades occupancy against rounds, so there are three shapes:
+//   0: uint32, 7 KB (9 warps per SM);
+//   1: uint32 batches of small blocks, 4752 bytes, the largest window at
+//      which 10 warps fit an SM (227 KB of shared memory, 1 KB reserved per
+//      CTA); chosen when the previous uint32 pack averaged at most
+//      kSmallBlock bytes a block;
+//   2: uint64, 10 KB: its tiles run to 32 sub-blocks of up to 528 bytes.
 constexpr int kWindow = 7168;
-constexpr int kImage = (kWindow + kMaxLen + 32 + 15) / 16 * 16;
-// The uint64 pack's tiles run to 32 sub-blocks of up to 528 bytes (two-block
-// shapes): a wider window keeps them to fewer rounds, at one warp less per SM.
+constexpr int kWindowSmall = 4752;
 constexpr int kWindow64 = 10240;
-constexpr int kImage64 = (kWindow64 + kMaxLen + 32 + 15) / 16 * 16;
-template <bool U64>
+constexpr int kSmallBlock = kWindowSmall / 32;
+template <int SHAPE>
 struct Window {
-  static constexpr int kBytes = U64 ? kWindow64 : kWindow;
-  static constexpr int kImageBytes = U64 ? kImage64 : kImage;
+  static constexpr int kBytes = SHAPE == 2 ? kWindow64 : (SHAPE == 1 ? kWindowSmall : kWindow);
+  static constexpr int kImageBytes = (kBytes + kMaxLen + 32 + 15) / 16 * 16;
 };
 
 // 4-bit bucket counter of a value: bucket b = clz/4 (zero values drop out).

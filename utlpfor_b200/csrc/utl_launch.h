@@ -19,6 +19,7 @@ struct PackArgs {
   unsigned long long* counter;  // tile work counter (scratch)
   uint64_t* tile_status;        // look-back states (scratch)
   uint32_t* err;
+  uint64_t* stats = nullptr;    // set by the launcher: packed bytes and blocks of the batch
 };
 
 struct UnpackArgs {
