@@ -282,7 +282,7 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *   UTL_KNOB_HOST_PIPELINE: the host-buffer batch calls, 0 = one pass
  *     (all copies in, kernels, all copies out); 1 = batches of 64 MiB of
  *     values or more are cut at block boundaries into pieces of
- *     max(32 MiB, batch/16) whose copies in, kernels and copies out overlap
+ *     max(16 MiB, batch/32) whose copies in, kernels and copies out overlap
  *     (the default); 2 = every batch in eighths (for tests).  Outputs are
  *     the same in every mode. */
 #define UTL_KNOB_UNPACK_SCHEDULE 0

@@ -93,7 +93,7 @@ struct HostGrow {
 };
 
 // Most pieces one host-buffer batch is cut into (one event pair each).
-constexpr int kMaxPieces = 32;
+constexpr int kMaxPieces = 64;
 
 struct Ctx {
   int device = 0;
@@ -585,17 +585,17 @@ static int first_error(uint32_t bits) {
 
 // Host-buffer batches go through the piecewise pipeline when the knob
 // allows: 0 = never, 1 = batches of at least kPipeMinBytes of values, in
-// pieces of max(kPieceMinBytes, batch / 16), 2 = any batch, in eighths.
+// pieces of max(kPieceMinBytes, batch / 32), 2 = any batch, in eighths.
 static std::atomic<int> g_host_pipe{1};
 constexpr uint64_t kPipeMinBytes = 64ull << 20;
-constexpr uint64_t kPieceMinBytes = 32ull << 20;
+constexpr uint64_t kPieceMinBytes = 16ull << 20;
 
 // Values per piece for a batch of nv values of esz bytes (0 = one piece).
 static uint64_t piece_target(uint64_t nv, size_t esz) {
   const uint64_t B = UTL_BLOCK_SIZE;
   const int mode = g_host_pipe.load(std::memory_order_relaxed);
   uint64_t t = 0;
-  if (mode == 1 && nv * esz >= kPipeMinBytes) t = std::max(kPieceMinBytes, nv * esz / 16) / esz;
+  if (mode == 1 && nv * esz >= kPipeMinBytes) t = std::max(kPieceMinBytes, nv * esz / 32) / esz;
   if (mode == 2) t = (nv + 7) / 8;
   return t ? (t + B - 1) / B * B : 0;
 }
