@@ -957,6 +957,9 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
 // taken, loaded, planned and published while the look-back loads of the
 // current one are in flight; finally the current tile's look-back is
 // finished and its image streamed to HBM at the resolved offset.
+// The uint64 pack runs the same loop over tiles of 16 uint64 blocks, a lane
+// pair per block and a lane per uint32 sub-block (SHAPE 2); the uint32 pack
+// picks its image window per launch (SHAPE 0 or 1, utl_lane.cuh).
 // ------------------------------------------------------------------------
 constexpr int kLWarps = 1;
 constexpr int kLThreads = kLWarps * 32;
