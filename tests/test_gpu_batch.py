@@ -48,7 +48,7 @@ def psched(request):
     L.utl_set_knob(2, old)
 
 
-@pytest.mark.parametrize("flag", range(8))
+@pytest.mark.parametrize("flag", list(range(8)) + [8, 9, 16, 49])
 @pytest.mark.parametrize("kind", ["small", "exc", "dense_exc", "sorted", "walk", "wide", "const", "zero", "full"])
 def test_pack_unpack_batch_u32(env, flag, kind, sched, psched):
     U, torch = env
