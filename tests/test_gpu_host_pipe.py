@@ -155,7 +155,8 @@ def test_corrupt_inputs_same_in_every_mode(L):
         set_mode(L, old)
 
 
-def test_large_batch_pieces_match_one_pass(L):
+@pytest.mark.parametrize("flag", [0, 1])
+def test_large_batch_pieces_match_one_pass(L, flag):
     """About 40 M values over 400 ragged streams (160 MB: the default mode
     cuts it into pieces, some inside streams): every output is the same as
     one pass, and the values come back."""
@@ -172,7 +173,7 @@ def test_large_batch_pieces_match_one_pass(L):
         res = {}
         for md in (0, 1):
             set_mode(L, md)
-            rc, got, bo, so, _ = c_pack(L, 0, v, vo)
+            rc, got, bo, so, _ = c_pack(L, flag, v, vo)
             assert rc == 0
             res[md] = (hashlib.sha256(got.tobytes()).digest(), bo, so)
             rc, out = c_unpack(L, got, bo, vo, np.uint32)
