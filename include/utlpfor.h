@@ -170,21 +170,27 @@ UTL_API int utl_pack_batch_u64(uint8_t flag, const uint64_t *d_values,
                        size_t scratch_bytes, uint32_t *d_err, void *stream);
 
 /* utl_pack_batch_u32 for callers that cannot allocate device memory while
- * they pack: work recorded into a CUDA graph (no allocation during stream
- * capture), latency-bound serving loops that cannot take the device-wide
+ * they pack: latency-bound serving loops that cannot take the device-wide
  * synchronisation of cudaMalloc/cudaFree, and hosts that own a fixed device
- * memory budget.  It has no counterpart in the reference (the Go library
+ * memory budget and hand out no allocation rights (a Go process calling
+ * through cgo that manages every device byte itself).  It has no counterpart in the reference (the Go library
  * never touches device memory).  Same arguments as utl_pack_batch_u32
  * without the scratch: the look-back tile states live in a 2 MiB array
  * built into the library, which every GPU that loads the library keeps
  * until the process exits.  Batches above
  * utl_pack_batch_u32_noalloc_max_blocks() blocks (about 4.2 million, i.e.
  * 5.4e8 values) are rejected with UTL_ERR_SCRATCH_LIMIT.  The first call
- * on a device looks up the array's device address (with that device
- * current); make that first call before any stream capture.  All calls on
- * a device share the array, so calls that overlap on the GPU (different
- * streams, or threads without ordering) race: serialise them.  Allocates
- * nothing and calls no allocating routine. */
+ * on a device (of this or any other batched entry point) sets the
+ * kernels' launch attributes and queries their occupancy on that device,
+ * and the first call of this entry point on a device looks up the array's
+ * device address (with that device current); make that first call before
+ * any stream capture.  The address lookup does not survive a
+ * cudaDeviceReset of that device.  All calls on a device share the array,
+ * so calls that overlap on the GPU (different streams, or threads without
+ * ordering) race: serialise them.  Calls no cudaMalloc, cudaFree,
+ * cudaHostAlloc or other allocating routine, on the first call too (the
+ * CUDA runtime itself may load the library's kernels onto the device on
+ * first use). */
 UTL_API int utl_pack_batch_u32_noalloc(uint8_t flag, const uint32_t *d_values,
                                const uint64_t *d_val_off,
                                const uint64_t *d_block_start, int n_streams,
@@ -284,11 +290,21 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *     values or more are cut at block boundaries into pieces of
  *     max(16 MiB, batch/32) whose copies in, kernels and copies out overlap
  *     (the default); 2 = every batch in eighths (for tests).  Outputs are
- *     the same in every mode. */
+ *     the same in every mode.
+ * Two knobs exist for tests of the pack's bounded waits only:
+ *   UTL_KNOB_SPIN_LIMIT: polls (64 ns sleep each) a waiting tile makes
+ *     before it gives up, records UTL_ERR_TIMEOUT in d_err and carries on
+ *     with a zero contribution (0 = the default, 2^22).
+ *   UTL_KNOB_KEEP_SCRATCH: 1 = the batched pack does not clear the caller's
+ *     scratch before its launch, so a test can preset the tile states
+ *     (for instance a work counter past tile 0, whose tile then never
+ *     publishes).  Output is undefined unless the scratch is zeroed. */
 #define UTL_KNOB_UNPACK_SCHEDULE 0
 #define UTL_KNOB_PACK_CTAS_PER_SM 1
 #define UTL_KNOB_PACK_SCHEDULE 2
 #define UTL_KNOB_HOST_PIPELINE 3
+#define UTL_KNOB_SPIN_LIMIT 4
+#define UTL_KNOB_KEEP_SCRATCH 5
 UTL_API int utl_set_knob(int knob, int value);
 UTL_API int utl_get_knob(int knob);
 

@@ -1039,3 +1039,44 @@ int utlo_unpack_streams_u64(const uint8_t *packed, const uint64_t *block_off, co
                             uint64_t *values, int n_threads) {
   return unpack_streams(1, packed, block_off, val_off, n_streams, values, n_threads);
 }
+
+/* Batched Get over packed streams: the block index of stream s's first
+ * block is the running sum of ceil(n/128) over the streams before it. */
+static void get_streams(int is64, const uint8_t *packed, const uint64_t *block_off, const uint64_t *val_off,
+                        int n_streams, const uint32_t *q_stream, const uint64_t *q_pos, int64_t n_queries, void *out,
+                        int32_t *status) {
+  int64_t *bs = block_starts(val_off, n_streams);
+  for (int64_t i = 0; i < n_queries; i++) {
+    const uint32_t s = q_stream[i];
+    const uint64_t p = q_pos[i];
+    int err = UTLO_ERR_POSITION_OUT_OF_RANGE, ovf = 0;
+    uint64_t v = 0;
+    if ((int64_t)s < n_streams && p < val_off[s + 1] - val_off[s]) {
+      const int64_t b = bs[s] + (int64_t)(p / BLOCK);
+      const uint8_t *blk = packed + block_off[b];
+      const size_t len = (size_t)(block_off[b + 1] - block_off[b]);
+      if (is64) {
+        err = utlo_get_u64((int)(p % BLOCK), blk, len, &v, &ovf);
+      } else {
+        uint32_t v32 = 0;
+        err = utlo_get_u32((int)(p % BLOCK), blk, len, &v32, &ovf);
+        v = v32;
+      }
+    }
+    if (is64) ((uint64_t *)out)[i] = err ? 0 : v;
+    else ((uint32_t *)out)[i] = err ? 0 : (uint32_t)v;
+    status[i] = err | (err == UTLO_ERR_OVERFLOW ? ovf << 8 : 0);
+  }
+  free(bs);
+}
+
+void utlo_get_streams_u32(const uint8_t *packed, const uint64_t *block_off, const uint64_t *val_off, int n_streams,
+                          const uint32_t *q_stream, const uint64_t *q_pos, int64_t n_queries, uint32_t *out,
+                          int32_t *status) {
+  get_streams(0, packed, block_off, val_off, n_streams, q_stream, q_pos, n_queries, out, status);
+}
+void utlo_get_streams_u64(const uint8_t *packed, const uint64_t *block_off, const uint64_t *val_off, int n_streams,
+                          const uint32_t *q_stream, const uint64_t *q_pos, int64_t n_queries, uint64_t *out,
+                          int32_t *status) {
+  get_streams(1, packed, block_off, val_off, n_streams, q_stream, q_pos, n_queries, out, status);
+}

@@ -100,6 +100,18 @@ int utlo_unpack_streams_u64(const uint8_t *packed, const uint64_t *block_off,
                             const uint64_t *val_off, int n_streams,
                             uint64_t *values, int n_threads);
 
+/* GetUint32/GetUint64 for n_queries (stream, position-in-stream) pairs
+ * over packed streams laid out as utlo_pack_streams writes them: query i
+ * reads block pos/128 of stream q_stream[i] and calls utlo_get_u32/u64 on
+ * it.  status[i] = error | (overflow position << 8); a stream or position
+ * out of range is UTLO_ERR_POSITION_OUT_OF_RANGE. */
+void utlo_get_streams_u32(const uint8_t *packed, const uint64_t *block_off, const uint64_t *val_off, int n_streams,
+                          const uint32_t *q_stream, const uint64_t *q_pos, int64_t n_queries, uint32_t *out,
+                          int32_t *status);
+void utlo_get_streams_u64(const uint8_t *packed, const uint64_t *block_off, const uint64_t *val_off, int n_streams,
+                          const uint32_t *q_stream, const uint64_t *q_pos, int64_t n_queries, uint64_t *out,
+                          int32_t *status);
+
 #ifdef __cplusplus
 }
 #endif

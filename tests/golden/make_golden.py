@@ -1,7 +1,7 @@
 """Regenerate tests/golden/golden.json from the reference's test data.
 
-Run once in a checkout that has the reference tree (default path given by
---ref).  The output is committed, so the tests never read the reference.
+Run once where a checkout of the reference module exists, passing its path
+with --ref (required).  The output is committed, so the tests never read the reference.
 
 What it records:
   * the four byte-exact golden blocks of testdata/*.bin together with the
@@ -88,7 +88,7 @@ def examples():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="checkout of the reference module (its testdata/ is read)")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "golden.json"))
     a = ap.parse_args()
     td = os.path.join(a.ref, "testdata")

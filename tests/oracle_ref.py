@@ -47,6 +47,11 @@ def lib():
         L.utlo_pack_streams_u64.argtypes = [C.c_uint8, PU64, PU64, C.c_int, P8, C.c_size_t, PU64, PU64, C.c_int]
         L.utlo_unpack_streams_u32.argtypes = [P8, PU64, PU64, C.c_int, PU32, C.c_int]
         L.utlo_unpack_streams_u64.argtypes = [P8, PU64, PU64, C.c_int, PU64, C.c_int]
+        PI32 = C.POINTER(C.c_int32)
+        L.utlo_get_streams_u32.argtypes = [P8, PU64, PU64, C.c_int, PU32, PU64, C.c_int64, PU32, PI32]
+        L.utlo_get_streams_u32.restype = None
+        L.utlo_get_streams_u64.argtypes = [P8, PU64, PU64, C.c_int, PU32, PU64, C.c_int64, PU64, PI32]
+        L.utlo_get_streams_u64.restype = None
         _lib = L
     return _lib
 
@@ -169,6 +174,23 @@ def unpack_streams(packed, block_off, val_off, dtype=np.uint32, n_threads=4):
         err = L.utlo_unpack_streams_u32(_p(pk, C.c_uint8), _p(bo, C.c_uint64), _p(vo, C.c_uint64), len(vo) - 1,
                                         _p(out, C.c_uint32), n_threads)
     return out, err
+
+
+def get_streams(packed, block_off, val_off, q_stream, q_pos, is64=False):
+    """GetUint32/GetUint64 per (stream, position) query over packed
+    streams: (values, status = error | overflow position << 8)."""
+    L = lib()
+    vo = np.ascontiguousarray(val_off, dtype=np.uint64)
+    bo = np.ascontiguousarray(block_off, dtype=np.uint64)
+    pk = np.ascontiguousarray(packed, dtype=np.uint8)
+    qs = np.ascontiguousarray(q_stream, dtype=np.uint32)
+    qp = np.ascontiguousarray(q_pos, dtype=np.uint64)
+    out = np.zeros(qs.size, dtype=np.uint64 if is64 else np.uint32)
+    st = np.zeros(qs.size, dtype=np.int32)
+    fn = L.utlo_get_streams_u64 if is64 else L.utlo_get_streams_u32
+    fn(_p(pk, C.c_uint8), _p(bo, C.c_uint64), _p(vo, C.c_uint64), len(vo) - 1, _p(qs, C.c_uint32),
+       _p(qp, C.c_uint64), qs.size, _p(out, C.c_uint64 if is64 else C.c_uint32), _p(st, C.c_int32))
+    return out, st
 
 
 def index_stream(packed):

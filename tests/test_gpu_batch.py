@@ -48,9 +48,26 @@ def psched(request):
     L.utl_set_knob(2, old)
 
 
-@pytest.mark.parametrize("flag", list(range(8)) + [8, 9, 16, 49])
-@pytest.mark.parametrize("kind", ["small", "exc", "dense_exc", "sorted", "walk", "wide", "const", "zero", "full"])
+KINDS = ["small", "exc", "dense_exc", "sorted", "walk", "wide", "const", "zero", "full"]
+
+
+@pytest.mark.parametrize("flag", list(range(16)))
+@pytest.mark.parametrize("kind", KINDS)
 def test_pack_unpack_batch_u32(env, flag, kind, sched, psched):
+    """Every combination of the four stored flag bits (Delta, NoFOR,
+    NoPatch, Special) under every pack and unpack schedule."""
+    _batch_u32_case(env, flag, kind)
+
+
+@pytest.mark.parametrize("flag", [f | extra for extra in (16, 32, 48) for f in range(16)])
+@pytest.mark.parametrize("kind", KINDS)
+def test_pack_unpack_batch_u32_placement_flags(env, flag, kind, psched):
+    """Append and NoInPlace (placement only: the same bytes) on top of every
+    stored-bit combination, under both pack schedules."""
+    _batch_u32_case(env, flag, kind)
+
+
+def _batch_u32_case(env, flag, kind):
     U, torch = env
     rng = np.random.default_rng(flag * 31 + len(kind))
     vals, vo = streams(rng, LENS, kind)
@@ -65,7 +82,7 @@ def test_pack_unpack_batch_u32(env, flag, kind, sched, psched):
     assert np.array_equal(out.cpu().numpy().view(np.uint32), vals)
 
 
-@pytest.mark.parametrize("flag", [0, 1, 2, 3, 4, 5, 6, 7, 8, 13])
+@pytest.mark.parametrize("flag", list(range(16)) + [16 | 5, 32 | 9, 48 | 15])
 @pytest.mark.parametrize("kind", ["for64", "full", "walk", "fit32", "upper_for", "zero"])
 def test_pack_unpack_batch_u64(env, flag, kind, psched):
     U, torch = env

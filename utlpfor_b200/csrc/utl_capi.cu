@@ -450,7 +450,9 @@ int utl_batch_plan(const uint64_t* d_val_off, int n_streams, uint64_t* d_block_s
 
 size_t utl_pack_scratch_bytes(int64_t n_blocks) { return launch::pack_scratch_bytes(n_blocks < 0 ? 0 : n_blocks); }
 
-static int pack_batch(bool u64, uint8_t flag, const void* d_values, const uint64_t* d_val_off,
+}  // extern "C"
+
+int utl::pack_batch_device(bool u64, bool may_alloc, uint8_t flag, const void* d_values, const uint64_t* d_val_off,
                       const uint64_t* d_block_start, int n_streams, int64_t n_blocks, uint8_t* d_out, size_t out_cap,
                       uint64_t* d_block_off, uint64_t* d_sbo, void* d_scratch, size_t scratch_bytes, uint32_t* d_err,
                       cudaStream_t st) {
@@ -461,7 +463,7 @@ static int pack_batch(bool u64, uint8_t flag, const void* d_values, const uint64
     UTL_CUDA(cudaMemsetAsync(d_block_off, 0, sizeof(uint64_t), st));
   } else {
     if (scratch_bytes < launch::pack_scratch_bytes(n_blocks)) return UTL_ERR_ARG;
-    UTL_CUDA(cudaMemsetAsync(d_scratch, 0, launch::pack_scratch_bytes(n_blocks), st));
+    if (!launch::keep_scratch()) UTL_CUDA(cudaMemsetAsync(d_scratch, 0, launch::pack_scratch_bytes(n_blocks), st));
     PackArgs a;
     a.values = d_values;
     a.val_off = d_val_off;
@@ -476,7 +478,8 @@ static int pack_batch(bool u64, uint8_t flag, const void* d_values, const uint64
     a.counter = (unsigned long long*)d_scratch;
     a.tile_status = (uint64_t*)((uint8_t*)d_scratch + 16);
     a.err = d_err;
-    cudaError_t e = launch::pack(u64, a, st);
+    a.spin_limit = launch::spin_limit();
+    cudaError_t e = launch::pack(u64, a, st, may_alloc);
     if (e != cudaSuccess) return cuda_fail(e);
   }
   if (d_sbo) {
@@ -486,19 +489,21 @@ static int pack_batch(bool u64, uint8_t flag, const void* d_values, const uint64
   return UTL_OK;
 }
 
+extern "C" {
+
 int utl_pack_batch_u32(uint8_t flag, const uint32_t* d_values, const uint64_t* d_val_off,
                        const uint64_t* d_block_start, int n_streams, int64_t n_blocks, uint8_t* d_out, size_t out_cap,
                        uint64_t* d_block_off, uint64_t* d_stream_byte_off, void* d_scratch, size_t scratch_bytes,
                        uint32_t* d_err, void* stream) {
-  return pack_batch(false, flag, d_values, d_val_off, d_block_start, n_streams, n_blocks, d_out, out_cap, d_block_off,
-                    d_stream_byte_off, d_scratch, scratch_bytes, d_err, (cudaStream_t)stream);
+  return pack_batch_device(false, true, flag, d_values, d_val_off, d_block_start, n_streams, n_blocks, d_out, out_cap,
+                           d_block_off, d_stream_byte_off, d_scratch, scratch_bytes, d_err, (cudaStream_t)stream);
 }
 int utl_pack_batch_u64(uint8_t flag, const uint64_t* d_values, const uint64_t* d_val_off,
                        const uint64_t* d_block_start, int n_streams, int64_t n_blocks, uint8_t* d_out, size_t out_cap,
                        uint64_t* d_block_off, uint64_t* d_stream_byte_off, void* d_scratch, size_t scratch_bytes,
                        uint32_t* d_err, void* stream) {
-  return pack_batch(true, flag, d_values, d_val_off, d_block_start, n_streams, n_blocks, d_out, out_cap, d_block_off,
-                    d_stream_byte_off, d_scratch, scratch_bytes, d_err, (cudaStream_t)stream);
+  return pack_batch_device(true, true, flag, d_values, d_val_off, d_block_start, n_streams, n_blocks, d_out, out_cap,
+                           d_block_off, d_stream_byte_off, d_scratch, scratch_bytes, d_err, (cudaStream_t)stream);
 }
 
 static int unpack_batch(bool u64, const uint8_t* d_packed, size_t packed_len, const uint64_t* d_block_off,
@@ -673,7 +678,7 @@ static int pack_streams_piped(Ctx* c, bool u64, uint8_t flag, const void* h_valu
     UTL_CUDA(cudaStreamWaitEvent(st, c->ev_in[k], 0));
     cudaError_t e = launch::plan(dtab + q.t0, q.ns, dbs + q.t0, st);
     if (e != cudaSuccess) return cuda_fail(e);
-    rc = pack_batch(u64, flag, dv, dtab + q.t0, dbs + q.t0, q.ns, n, (uint8_t*)c->packed.p + reg[k],
+    rc = pack_batch_device(u64, true, flag, dv, dtab + q.t0, dbs + q.t0, q.ns, n, (uint8_t*)c->packed.p + reg[k],
                     reg[k + 1] - reg[k], dbo + q.b0 + k, nullptr, c->scratch.p, c->scratch.cap, (uint32_t*)c->err.p,
                     st);
     if (rc != UTL_OK) return rc;
@@ -814,7 +819,7 @@ static int pack_streams(bool u64, uint8_t flag, const void* h_values, const uint
   }
   cudaError_t e = launch::plan(dvo, n_streams, (uint64_t*)c->bstart.p, st);
   if (e != cudaSuccess) return cuda_fail(e);
-  rc = pack_batch(u64, flag, c->values.p, dvo, (const uint64_t*)c->bstart.p, n_streams, nb, (uint8_t*)c->packed.p,
+  rc = pack_batch_device(u64, true, flag, c->values.p, dvo, (const uint64_t*)c->bstart.p, n_streams, nb, (uint8_t*)c->packed.p,
                   c->packed.cap, (uint64_t*)c->block_off.p, h_sbo ? (uint64_t*)c->sbo.p : nullptr, c->scratch.p,
                   c->scratch.cap, (uint32_t*)c->err.p, st);
   if (rc != UTL_OK) return rc;

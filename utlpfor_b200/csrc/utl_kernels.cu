@@ -15,6 +15,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <mutex>
+
 #include "utl_device.cuh"
 #include "utl_launch.h"
 #include "utl_lane.cuh"
@@ -208,11 +211,11 @@ __global__ void stream_off_kernel(const uint64_t* __restrict__ block_off, const 
 // batched pack with single-pass decoupled look-back
 // ------------------------------------------------------------------------
 // Tile state word: bits 0-1 flag (0 empty, 1 aggregate, 2 inclusive
-// prefix), bits 2-63 value.  Waits are bounded; on expiry the kernel
-// records UTL_ERR_TIMEOUT and carries on with a zero contribution so it
-// always terminates.  Tiles are handed out in launch order by an atomic
-// counter, so every predecessor of a waiting tile is already running.
-constexpr uint32_t kSpinLimit = 1u << 22;
+// prefix), bits 2-63 value.  Waits are bounded (PackArgs::spin_limit polls,
+// each after a 64 ns sleep); on expiry the kernel records UTL_ERR_TIMEOUT
+// and carries on with a zero contribution so it always terminates.  Tiles
+// are handed out in launch order by an atomic counter, so every
+// predecessor of a waiting tile is already running.
 
 // Each lane inspects 8 consecutive predecessors per round (lane 0 the 8
 // nearest), so one round covers 256 tiles: with hundreds of tiles in flight
@@ -226,7 +229,7 @@ __device__ __forceinline__ void tile_publish(uint64_t* status, int64_t tile, uin
 
 // Exclusive prefix of a tile whose aggregate is already published; then
 // publishes the tile's inclusive prefix.  Whole warp.
-__device__ uint64_t tile_resolve(uint64_t* status, int64_t tile, uint64_t agg, int lane, uint32_t* err) {
+__device__ uint64_t tile_resolve(uint64_t* status, int64_t tile, uint64_t agg, int lane, uint32_t* err, uint32_t lim) {
   if (tile == 0) return 0;
   uint64_t excl = 0;
   int64_t j = tile - 1;
@@ -243,7 +246,7 @@ __device__ uint64_t tile_resolve(uint64_t* status, int64_t tile, uint64_t agg, i
       const int64_t idx = j - (int64_t)lane * kLookPerLane - i;
       uint32_t it = 0;
       while ((st[i] & 3u) == 0) {
-        if (++it > kSpinLimit) {
+        if (++it > lim) {
           timed_out = true;
           st[i] = 2u;
           break;
@@ -287,7 +290,7 @@ __device__ __forceinline__ void tile_resolve_issue(const uint64_t* status, int64
 // Finish the look-back started by tile_resolve_issue (whole warp) and
 // publish the tile's inclusive prefix.
 __device__ __forceinline__ uint64_t tile_resolve_finish(uint64_t* status, int64_t tile, uint64_t agg, int lane,
-                                                       uint32_t* err, LookRound& r) {
+                                                       uint32_t* err, LookRound& r, uint32_t lim) {
   if (tile == 0) return 0;
   uint64_t excl = 0;
   int64_t j = tile - 1;
@@ -306,7 +309,7 @@ __device__ __forceinline__ uint64_t tile_resolve_finish(uint64_t* status, int64_
       const int64_t idx = j - (int64_t)lane * kLookPerLane - i;
       uint32_t it = 0;
       while ((st[i] & 3u) == 0) {
-        if (++it > kSpinLimit) {
+        if (++it > lim) {
           timed_out = true;
           st[i] = 2u;
           break;
@@ -337,15 +340,15 @@ __device__ __forceinline__ uint64_t tile_resolve_finish(uint64_t* status, int64_
 // Look-back of a tile whose aggregate is already published, in one go (out
 // of line: used only for tiles too large for the pack's image).
 __device__ __noinline__ uint64_t tile_resolve_now(uint64_t* status, int64_t tile, uint64_t agg, int lane,
-                                                  uint32_t* err) {
+                                                  uint32_t* err, uint32_t lim) {
   LookRound r;
   tile_resolve_issue(status, tile, lane, r);
-  return tile_resolve_finish(status, tile, agg, lane, err, r);
+  return tile_resolve_finish(status, tile, agg, lane, err, r, lim);
 }
 
-__device__ uint64_t tile_lookback(uint64_t* status, int64_t tile, uint64_t agg, int lane, uint32_t* err) {
+__device__ uint64_t tile_lookback(uint64_t* status, int64_t tile, uint64_t agg, int lane, uint32_t* err, uint32_t lim) {
   if (lane == 0) tile_publish(status, tile, agg);
-  return tile_resolve(status, tile, agg, lane, err);
+  return tile_resolve(status, tile, agg, lane, err, lim);
 }
 
 template <bool U64>
@@ -400,7 +403,7 @@ __global__ void __launch_bounds__(kThreads) pack_kernel(PackArgs a) {
       const int incl = warp_incl_scan(l, lane);
       if (lane < kTile) s_off[lane] = incl - l;
       const uint64_t agg = (uint64_t)__shfl_sync(kFull, incl, 31);
-      const uint64_t prefix = tile_lookback(a.tile_status, tile, agg, lane, a.err);
+      const uint64_t prefix = tile_lookback(a.tile_status, tile, agg, lane, a.err, a.spin_limit);
       if (lane == 0) s_prefix = prefix;
     }
     __syncthreads();
@@ -890,7 +893,7 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
         }
       }
       if (ptile >= 0) {
-        const uint64_t pre = tile_resolve_finish(a.tile_status, ptile, (uint64_t)S.off[pb][kQTile], lane, a.err, lr);
+        const uint64_t pre = tile_resolve_finish(a.tile_status, ptile, (uint64_t)S.off[pb][kQTile], lane, a.err, lr, a.spin_limit);
         if (lane == 0) S.prefix = pre;
       }
     }
@@ -902,7 +905,7 @@ __global__ void __launch_bounds__(kQThreads, 4) pack_quad_kernel(PackArgs a) {
     const bool direct = total > kQImage;
     if (direct) {
       if (warp == 0) {
-        const uint64_t pre = tile_resolve_now(a.tile_status, tile, (uint64_t)total, lane, a.err);
+        const uint64_t pre = tile_resolve_now(a.tile_status, tile, (uint64_t)total, lane, a.err, a.spin_limit);
         if (lane == 0) S.direct_prefix = pre;
       }
       __syncthreads();
@@ -1188,6 +1191,7 @@ __device__ __forceinline__ Shape64 lane_shape64(uint8_t* inb, int nk, int flag, 
 struct LaneScan {
   uint32_t* agg;  // n_tiles words
   uint32_t* grp;  // ceil(n_tiles / 32) words
+  uint32_t lim;   // spin limit of each wait
 };
 __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
   uint32_t v;
@@ -1227,7 +1231,7 @@ __device__ __forceinline__ void lane_win_issue(const LaneScan& sc, int64_t lo, i
 }
 __device__ __forceinline__ uint32_t lane_wait_tile(const LaneScan& sc, int64_t j, uint32_t v, bool& to) {
   for (uint32_t it = 0; v == 0; it++) {
-    if (it > kSpinLimit) {
+    if (it > sc.lim) {
       to = true;
       return 1u;
     }
@@ -1238,7 +1242,7 @@ __device__ __forceinline__ uint32_t lane_wait_tile(const LaneScan& sc, int64_t j
 }
 __device__ __forceinline__ uint32_t lane_wait_group(const LaneScan& sc, int64_t g, uint32_t v, bool& to) {
   for (uint32_t it = 0; (v & 63u) != 32u; it++) {
-    if (it > kSpinLimit) {
+    if (it > sc.lim) {
       to = true;
       return 32u;
     }
@@ -1388,6 +1392,7 @@ __global__ void __launch_bounds__(kLThreads, 8) pack_lane_kernel(PackArgs a) {
   LaneScan sc;
   sc.agg = (uint32_t*)a.tile_status;
   sc.grp = sc.agg + a.n_tiles;
+  sc.lim = a.spin_limit;
   int64_t prev = -1;       // the last tile this warp finished
   uint64_t prev_incl = 0;  // its inclusive prefix
   // the current tile (planned and published; -1: none yet) and its layout
@@ -1737,17 +1742,92 @@ __global__ void __launch_bounds__(32) plain_get_kernel(int pos, const uint8_t* s
 // ------------------------------------------------------------------------
 namespace launch {
 
-static int g_num_sms = 0;
-static int g_pack_ctas_per_sm[2] = {0, 0};
+// Launch configuration of one device: kernel attributes set and resident
+// CTAs per SM queried once per device (with that device current), under a
+// lock, and published through `ready` only after every field is written.
+// Setting attributes and querying occupancy allocates nothing (the CUDA
+// runtime may load this library's kernels onto the device the first time).
+constexpr int kMaxDevices = 64;
+struct DevCfg {
+  std::atomic<int> ready{0};
+  cudaError_t err = cudaSuccess;
+  int sms = 0;
+  int lane_ctas[3] = {0, 0, 0};  // pack_lane_kernel, per window shape
+  int quad_pack_ctas = 0;        // pack_quad_kernel
+  int pipe_ctas = 0;             // unpack_quad_pipe_kernel, narrow staging
+  int pipe_wide_ctas = 0;        // unpack_quad_pipe_kernel, wide staging
+  int pack_ctas[2] = {0, 0};     // pack_kernel<false/true>
+  // Mapped pinned pair the uint32 lane pack's last block fills with the
+  // batch's packed bytes and block count; the next allocating launch on
+  // this device reads it (without waiting) to pick its window shape.  Only
+  // a performance hint: a stale or torn pair picks the other shape, whose
+  // output is the same.  Allocated by the first pack that may allocate.
+  std::atomic<uint64_t*> stats{nullptr};
+  uint64_t* stats_dev = nullptr;
+};
+static DevCfg g_dev[kMaxDevices];
+static std::mutex g_setup_mu;
+
+template <class K>
+static cudaError_t set_smem(K kern, size_t bytes) {
+  cudaError_t e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return e;
+  cudaFuncSetAttribute((const void*)kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  return cudaSuccess;
+}
+template <class K>
+static int occupancy(K kern, int threads, size_t bytes) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, bytes) != cudaSuccess || n <= 0) n = 1;
+  return n;
+}
+
+static cudaError_t setup_device(int dev, DevCfg& c);
+
+// The current device's configuration, set up on first use.
+static cudaError_t dev_cfg(DevCfg** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  DevCfg& c = g_dev[dev];
+  if (!c.ready.load(std::memory_order_acquire)) {
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    if (!c.ready.load(std::memory_order_relaxed)) {
+      e = setup_device(dev, c);
+      if (e != cudaSuccess) return e;
+      c.ready.store(1, std::memory_order_release);
+    }
+  }
+  *out = &c;
+  return cudaSuccess;
+}
+
+// The mapped pinned stats pair of a device (allocating; once per device).
+static uint64_t* lane_stats_dev(DevCfg& c) {
+  if (c.stats.load(std::memory_order_acquire)) return c.stats_dev;
+  std::lock_guard<std::mutex> lk(g_setup_mu);
+  if (c.stats.load(std::memory_order_relaxed)) return c.stats_dev;
+  uint64_t* h = nullptr;
+  if (cudaHostAlloc((void**)&h, 2 * sizeof(uint64_t), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  h[0] = h[1] = 0;
+  uint64_t* d = nullptr;
+  if (cudaHostGetDevicePointer((void**)&d, h, 0) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFreeHost(h);
+    return nullptr;
+  }
+  c.stats_dev = d;
+  c.stats.store(h, std::memory_order_release);
+  return d;
+}
 
 static int num_sms() {
-  if (g_num_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 148;
-  }
-  return g_num_sms;
+  DevCfg* c = nullptr;
+  return dev_cfg(&c) == cudaSuccess ? c->sms : 148;
 }
 
 size_t pack_smem(bool u64) {
@@ -1772,89 +1852,88 @@ cudaError_t stream_offsets(const uint64_t* block_off, const uint64_t* bstart, in
   return cudaGetLastError();
 }
 
-static int g_quad_pack_ctas = 0;
-static bool g_quad_unpack_cfg = false;
-static int g_pipe_ctas = 0;
-static int g_pipe_wide_ctas = 0;
-
 template <int STAGE, bool AUTO>
-static cudaError_t unpack_pipe(const UnpackArgs& a, cudaStream_t st, int& ctas) {
+static cudaError_t unpack_pipe(const UnpackArgs& a, cudaStream_t st, int ctas) {
   const size_t psmem = sizeof(QuadPipeSmem<STAGE>);
-  auto kern = unpack_quad_pipe_kernel<STAGE, AUTO>;
-  if (ctas == 0) {
-    for (const void* f : {(const void*)unpack_quad_pipe_kernel<STAGE, true>,
-                          (const void*)unpack_quad_pipe_kernel<STAGE, false>}) {
-      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
-      if (e != cudaSuccess) return e;
-      cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kern, kQThreads, psmem);
-    if (ctas <= 0) ctas = 1;
-  }
   const int64_t groups = (a.n_blocks + 7) / 8;
   int64_t grid = (int64_t)num_sms() * ctas;
   const int64_t need = (groups + kQWarps - 1) / kQWarps;
   if (grid > need) grid = need;
-  kern<<<(unsigned)grid, kQThreads, psmem, st>>>(a);
+  unpack_quad_pipe_kernel<STAGE, AUTO><<<(unsigned)grid, kQThreads, psmem, st>>>(a);
   note_launch(1);
   return cudaGetLastError();
 }
 // 0: one CTA per 32 blocks; 1: persistent pipelined warps (selectable for tuning)
 static int g_unpack_schedule = 1;
 static int g_pack_cap = 0;
-
 static int g_pack_schedule = 1;
-static int g_lane_ctas[3] = {0, 0, 0};  // resident CTAs per SM of each window shape
-// Mapped pinned words the uint32 lane pack's last block fills with the
-// batch's packed bytes and block count; the next launch reads them (without
-// waiting) to pick its window shape.  Only a performance hint: a stale or
-// torn pair picks the other shape, whose output is the same.
-static uint64_t* g_lane_stats = nullptr;
-static uint64_t* g_lane_stats_dev = nullptr;
+// Test knobs: the polls of every bounded wait (0 = the default 2^22), and
+// whether the pack leaves the caller's scratch as it finds it.
+static std::atomic<uint32_t> g_spin_limit{0};
+static std::atomic<int> g_keep_scratch{0};
+uint32_t spin_limit() {
+  const uint32_t v = g_spin_limit.load(std::memory_order_relaxed);
+  return v ? v : (1u << 22);
+}
+bool keep_scratch() { return g_keep_scratch.load(std::memory_order_relaxed) != 0; }
 
 template <bool DELTA, int SHAPE>
 static void launch_lane(const PackArgs& a, int64_t grid, cudaStream_t st) {
   pack_lane_kernel<DELTA, SHAPE><<<(unsigned)grid, kLThreads, sizeof(LaneWarpSmem<SHAPE>) * kLWarps, st>>>(a);
 }
 
-static cudaError_t pack_lane(const PackArgs& a_in, cudaStream_t st, bool u64) {
+static cudaError_t setup_device(int dev, DevCfg& c) {
+  cudaError_t e = cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  if (c.sms <= 0) c.sms = 148;
+  const size_t lsm[3] = {sizeof(LaneWarpSmem<0>) * kLWarps, sizeof(LaneWarpSmem<1>) * kLWarps,
+                         sizeof(LaneWarpSmem<2>) * kLWarps};
+  if ((e = set_smem(pack_lane_kernel<false, 0>, lsm[0])) != cudaSuccess) return e;
+  if ((e = set_smem(pack_lane_kernel<true, 0>, lsm[0])) != cudaSuccess) return e;
+  if ((e = set_smem(pack_lane_kernel<false, 1>, lsm[1])) != cudaSuccess) return e;
+  if ((e = set_smem(pack_lane_kernel<true, 1>, lsm[1])) != cudaSuccess) return e;
+  if ((e = set_smem(pack_lane_kernel<false, 2>, lsm[2])) != cudaSuccess) return e;
+  if ((e = set_smem(pack_lane_kernel<true, 2>, lsm[2])) != cudaSuccess) return e;
+  c.lane_ctas[0] = occupancy(pack_lane_kernel<false, 0>, kLThreads, lsm[0]);
+  c.lane_ctas[1] = occupancy(pack_lane_kernel<false, 1>, kLThreads, lsm[1]);
+  c.lane_ctas[2] = occupancy(pack_lane_kernel<false, 2>, kLThreads, lsm[2]);
+  if ((e = set_smem(pack_quad_kernel, sizeof(QuadPackSmem))) != cudaSuccess) return e;
+  c.quad_pack_ctas = occupancy(pack_quad_kernel, kQThreads, sizeof(QuadPackSmem));
+  if ((e = set_smem(pack_kernel<false>, pack_smem(false))) != cudaSuccess) return e;
+  if ((e = set_smem(pack_kernel<true>, pack_smem(true))) != cudaSuccess) return e;
+  c.pack_ctas[0] = occupancy(pack_kernel<false>, kThreads, pack_smem(false));
+  c.pack_ctas[1] = occupancy(pack_kernel<true>, kThreads, pack_smem(true));
+  if ((e = set_smem(unpack_quad_kernel, sizeof(QuadUnpackSmem))) != cudaSuccess) return e;
+  const size_t pn = sizeof(QuadPipeSmem<kPStageNarrow>), pw = sizeof(QuadPipeSmem<kPStageWide>);
+  if ((e = set_smem(unpack_quad_pipe_kernel<kPStageNarrow, true>, pn)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_pipe_kernel<kPStageNarrow, false>, pn)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_pipe_kernel<kPStageWide, true>, pw)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_pipe_kernel<kPStageWide, false>, pw)) != cudaSuccess) return e;
+  c.pipe_ctas = occupancy(unpack_quad_pipe_kernel<kPStageNarrow, false>, kQThreads, pn);
+  c.pipe_wide_ctas = occupancy(unpack_quad_pipe_kernel<kPStageWide, false>, kQThreads, pw);
+  if ((e = set_smem(unpack_kernel<false>, unpack_smem(false))) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_kernel<true>, unpack_smem(true))) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+static cudaError_t pack_lane(const PackArgs& a_in, cudaStream_t st, bool u64, bool may_alloc, DevCfg& c) {
   PackArgs a = a_in;
   a.n_tiles = u64 ? (a.n_blocks + 15) / 16 : (a.n_blocks + 31) / 32;
-  if (g_lane_ctas[0] == 0) {
-    const void* fs[6] = {(const void*)pack_lane_kernel<false, 0>, (const void*)pack_lane_kernel<true, 0>,
-                         (const void*)pack_lane_kernel<false, 1>, (const void*)pack_lane_kernel<true, 1>,
-                         (const void*)pack_lane_kernel<false, 2>, (const void*)pack_lane_kernel<true, 2>};
-    const size_t sms[3] = {sizeof(LaneWarpSmem<0>) * kLWarps, sizeof(LaneWarpSmem<1>) * kLWarps,
-                           sizeof(LaneWarpSmem<2>) * kLWarps};
-    for (int i = 0; i < 6; i++) {
-      cudaError_t e = cudaFuncSetAttribute(fs[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms[i / 2]);
-      if (e != cudaSuccess) return e;
-      cudaFuncSetAttribute(fs[i], cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    }
-    for (int sh = 0; sh < 3; sh++) {
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_lane_ctas[sh], fs[2 * sh], kLThreads, sms[sh]);
-      if (g_lane_ctas[sh] <= 0) g_lane_ctas[sh] = 1;
-    }
-    if (cudaHostAlloc((void**)&g_lane_stats, 2 * sizeof(uint64_t), cudaHostAllocMapped | cudaHostAllocPortable) ==
-        cudaSuccess) {
-      g_lane_stats[0] = g_lane_stats[1] = 0;
-      if (cudaHostGetDevicePointer((void**)&g_lane_stats_dev, g_lane_stats, 0) != cudaSuccess)
-        g_lane_stats_dev = nullptr;
-    } else {
-      g_lane_stats = nullptr;
-      cudaGetLastError();
-    }
-  }
   int shape = 2;
+  a.stats = nullptr;
   if (!u64) {
-    const volatile uint64_t* sv = g_lane_stats;
-    const uint64_t bytes = sv ? sv[0] : 0, blocks = sv ? sv[1] : 0;
-    shape = (blocks > 0 && bytes <= blocks * (uint64_t)lane::kSmallBlock) ? 1 : 0;
-    a.stats = g_lane_stats_dev;
+    shape = 0;
+    const uint64_t* sv = may_alloc ? lane_stats_dev(c) : nullptr;
+    if (sv) {
+      const volatile uint64_t* hv = c.stats.load(std::memory_order_acquire);
+      const uint64_t bytes = hv[0], blocks = hv[1];
+      shape = (blocks > 0 && bytes <= blocks * (uint64_t)lane::kSmallBlock) ? 1 : 0;
+      a.stats = c.stats_dev;
+    }
   }
-  const int occ = g_lane_ctas[shape];
+  const int occ = c.lane_ctas[shape];
   const int per_sm = (g_pack_cap > 0 && g_pack_cap < occ) ? g_pack_cap : occ;
-  int64_t grid = (int64_t)num_sms() * per_sm;
+  int64_t grid = (int64_t)c.sms * per_sm;
   if (grid * kLWarps > a.n_tiles) grid = (a.n_tiles + kLWarps - 1) / kLWarps;
   if (grid < 1) grid = 1;
   const bool d = (a.flag & kDelta) != 0;
@@ -1867,87 +1946,51 @@ static cudaError_t pack_lane(const PackArgs& a_in, cudaStream_t st, bool u64) {
   return cudaGetLastError();
 }
 
-cudaError_t pack(bool u64, const PackArgs& a_in, cudaStream_t st) {
-  if (g_pack_schedule == 1) return pack_lane(a_in, st, u64);
+cudaError_t pack(bool u64, const PackArgs& a_in, cudaStream_t st, bool may_alloc) {
+  DevCfg* c = nullptr;
+  cudaError_t e = dev_cfg(&c);
+  if (e != cudaSuccess) return e;
+  if (g_pack_schedule == 1) return pack_lane(a_in, st, u64, may_alloc, *c);
   if (!u64) {
     PackArgs a = a_in;
     a.n_tiles = (a.n_blocks + kQTile - 1) / kQTile;
-    const size_t smem = sizeof(QuadPackSmem);
-    if (g_quad_pack_ctas == 0) {
-      cudaError_t e = cudaFuncSetAttribute(pack_quad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      cudaFuncSetAttribute(pack_quad_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_quad_pack_ctas, pack_quad_kernel, kQThreads, smem);
-      if (g_quad_pack_ctas <= 0) g_quad_pack_ctas = 1;
-    }
-    const int per_sm = (g_pack_cap > 0 && g_pack_cap < g_quad_pack_ctas) ? g_pack_cap : g_quad_pack_ctas;
-    int64_t grid = (int64_t)num_sms() * per_sm;
+    const int per_sm = (g_pack_cap > 0 && g_pack_cap < c->quad_pack_ctas) ? g_pack_cap : c->quad_pack_ctas;
+    int64_t grid = (int64_t)c->sms * per_sm;
     if (grid > a.n_tiles) grid = a.n_tiles;
     if (grid < 1) grid = 1;
-    pack_quad_kernel<<<(unsigned)grid, kQThreads, smem, st>>>(a);
+    pack_quad_kernel<<<(unsigned)grid, kQThreads, sizeof(QuadPackSmem), st>>>(a);
     note_launch(1);
     return cudaGetLastError();
   }
   const PackArgs& a = a_in;
-  const size_t smem = pack_smem(u64);
-  const int idx = u64 ? 1 : 0;
-  if (g_pack_ctas_per_sm[idx] == 0) {
-    cudaError_t e;
-    if (u64) {
-      e = cudaFuncSetAttribute(pack_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_pack_ctas_per_sm[idx], pack_kernel<true>, kThreads, smem);
-    } else {
-      e = cudaFuncSetAttribute(pack_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_pack_ctas_per_sm[idx], pack_kernel<false>, kThreads, smem);
-    }
-    if (g_pack_ctas_per_sm[idx] <= 0) g_pack_ctas_per_sm[idx] = 1;
-  }
-  int64_t grid = (int64_t)num_sms() * g_pack_ctas_per_sm[idx];
+  int64_t grid = (int64_t)c->sms * c->pack_ctas[1];
   if (grid > a.n_tiles) grid = a.n_tiles;
   if (grid < 1) grid = 1;
-  if (u64) pack_kernel<true><<<(unsigned)grid, kThreads, smem, st>>>(a);
-  else pack_kernel<false><<<(unsigned)grid, kThreads, smem, st>>>(a);
+  pack_kernel<true><<<(unsigned)grid, kThreads, pack_smem(true), st>>>(a);
   note_launch(1);
   return cudaGetLastError();
 }
 
 cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
+  if (a.n_blocks <= 0) return cudaSuccess;
+  DevCfg* c = nullptr;
+  cudaError_t e = dev_cfg(&c);
+  if (e != cudaSuccess) return e;
   if (!u64) {
-    const size_t smem = sizeof(QuadUnpackSmem);
-    if (!g_quad_unpack_cfg) {
-      cudaError_t e = cudaFuncSetAttribute(unpack_quad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      cudaFuncSetAttribute(unpack_quad_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-      g_quad_unpack_cfg = true;
-    }
-    if (a.n_blocks <= 0) return cudaSuccess;
     if (g_unpack_schedule == 1) {  // by the batch's mean block length, decided on the device
-      cudaError_t e = unpack_pipe<kPStageNarrow, true>(a, st, g_pipe_ctas);
+      e = unpack_pipe<kPStageNarrow, true>(a, st, c->pipe_ctas);
       if (e != cudaSuccess) return e;
-      return unpack_pipe<kPStageWide, true>(a, st, g_pipe_wide_ctas);
+      return unpack_pipe<kPStageWide, true>(a, st, c->pipe_wide_ctas);
     }
-    if (g_unpack_schedule == 2) return unpack_pipe<kPStageWide, false>(a, st, g_pipe_wide_ctas);
-    if (g_unpack_schedule == 3) return unpack_pipe<kPStageNarrow, false>(a, st, g_pipe_ctas);
+    if (g_unpack_schedule == 2) return unpack_pipe<kPStageWide, false>(a, st, c->pipe_wide_ctas);
+    if (g_unpack_schedule == 3) return unpack_pipe<kPStageNarrow, false>(a, st, c->pipe_ctas);
     const int64_t grid = (a.n_blocks + kQTile - 1) / kQTile;
-    unpack_quad_kernel<<<(unsigned)grid, kQThreads, smem, st>>>(a);
+    unpack_quad_kernel<<<(unsigned)grid, kQThreads, sizeof(QuadUnpackSmem), st>>>(a);
     note_launch(1);
     return cudaGetLastError();
   }
-  const size_t smem = unpack_smem(u64);
-  static bool configured[2] = {false, false};
-  const int idx = u64 ? 1 : 0;
-  if (!configured[idx]) {
-    cudaError_t e = u64 ? cudaFuncSetAttribute(unpack_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                        : cudaFuncSetAttribute(unpack_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured[idx] = true;
-  }
   const int64_t grid = tiles_for(a.n_blocks);
-  if (grid <= 0) return cudaSuccess;
-  if (u64) unpack_kernel<true><<<(unsigned)grid, kThreads, smem, st>>>(a);
-  else unpack_kernel<false><<<(unsigned)grid, kThreads, smem, st>>>(a);
+  unpack_kernel<true><<<(unsigned)grid, kThreads, unpack_smem(true), st>>>(a);
   note_launch(1);
   return cudaGetLastError();
 }
@@ -1998,6 +2041,14 @@ int set_knob(int knob, int value) {
       if (value != 0 && value != 1) return -1;
       g_pack_schedule = value;
       return 0;
+    case 4:  // UTL_KNOB_SPIN_LIMIT (0 = default)
+      if (value < 0 || value > (1 << 30)) return -1;
+      g_spin_limit.store((uint32_t)value, std::memory_order_relaxed);
+      return 0;
+    case 5:  // UTL_KNOB_KEEP_SCRATCH
+      if (value != 0 && value != 1) return -1;
+      g_keep_scratch.store(value, std::memory_order_relaxed);
+      return 0;
   }
   return -1;
 }
@@ -2006,6 +2057,8 @@ int get_knob(int knob) {
     case 0: return g_unpack_schedule;
     case 1: return g_pack_cap;
     case 2: return g_pack_schedule;
+    case 4: return (int)g_spin_limit.load(std::memory_order_relaxed);
+    case 5: return g_keep_scratch.load(std::memory_order_relaxed);
   }
   return -1;
 }

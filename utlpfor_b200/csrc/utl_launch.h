@@ -20,6 +20,7 @@ struct PackArgs {
   uint64_t* tile_status;        // look-back states (scratch)
   uint32_t* err;
   uint64_t* stats = nullptr;    // set by the launcher: packed bytes and blocks of the batch
+  uint32_t spin_limit = 1u << 22;  // polls of each bounded wait (UTL_KNOB_SPIN_LIMIT)
 };
 
 struct UnpackArgs {
@@ -62,6 +63,13 @@ struct PlainResult {
 
 void note_launch(int n);
 
+// The batched pack behind utl_pack_batch_u32/u64 (argument checks, scratch
+// clearing, launch); may_alloc as for launch::pack.  Returns a UTL_* status.
+int pack_batch_device(bool u64, bool may_alloc, uint8_t flag, const void* d_values, const uint64_t* d_val_off,
+                      const uint64_t* d_block_start, int n_streams, int64_t n_blocks, uint8_t* d_out, size_t out_cap,
+                      uint64_t* d_block_off, uint64_t* d_sbo, void* d_scratch, size_t scratch_bytes, uint32_t* d_err,
+                      cudaStream_t st);
+
 namespace launch {
 size_t pack_smem(bool u64);
 size_t unpack_smem(bool u64);
@@ -70,7 +78,9 @@ int64_t tiles_for(int64_t n_blocks);
 inline size_t pack_scratch_bytes(int64_t n_blocks) { return 16 + 8 * (size_t)tiles_for(n_blocks); }
 cudaError_t plan(const uint64_t* val_off, int n, uint64_t* bstart, cudaStream_t st);
 cudaError_t stream_offsets(const uint64_t* block_off, const uint64_t* bstart, int n, uint64_t* sbo, cudaStream_t st);
-cudaError_t pack(bool u64, const PackArgs& a, cudaStream_t st);
+// may_alloc false: the launch makes no allocation of any kind (the uint32
+// lane pack then skips its mapped-memory window hint).
+cudaError_t pack(bool u64, const PackArgs& a, cudaStream_t st, bool may_alloc);
 cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st);
 cudaError_t get(bool u64, const GetArgs& a, cudaStream_t st);
 cudaError_t plain_pack(bool u64, int flag, const void* vals, int n, uint8_t* out, PlainResult* res, cudaStream_t st);
@@ -83,5 +93,7 @@ int index_stream(const uint8_t* p, uint64_t len, uint64_t* block_off, int64_t ma
                  void* scratch, cudaStream_t st, cudaError_t* cerr);
 int set_knob(int knob, int value);
 int get_knob(int knob);
+uint32_t spin_limit();     // UTL_KNOB_SPIN_LIMIT as a poll count
+bool keep_scratch();       // UTL_KNOB_KEEP_SCRATCH
 }  // namespace launch
 }  // namespace utl

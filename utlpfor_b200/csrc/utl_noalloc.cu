@@ -1,11 +1,10 @@
 // utl_noalloc.cu -- batched pack that allocates nothing.
 //
-// Some callers cannot allocate device memory when they pack: code that
-// records its work into a CUDA graph (allocation is not allowed while a
-// stream is being captured), serving loops whose latency budget cannot
-// absorb the device-wide synchronisation a cudaMalloc/cudaFree may cause,
-// and hosts that hand this library a fixed memory budget up front (a Go
-// process calling through cgo that manages every device byte itself).
+// Some callers cannot allocate device memory when they pack: serving loops
+// whose latency budget cannot absorb the device-wide synchronisation a
+// cudaMalloc/cudaFree may cause, and hosts that hand this library a fixed
+// memory budget up front (a Go process calling through cgo that manages
+// every device byte itself).
 // utl_pack_batch_u32_noalloc serves them: the caller passes only inputs and
 // outputs, and the look-back tile states live in the fixed-size array
 // below instead of caller-provided or library-allocated scratch.
@@ -30,7 +29,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-void* g_addr[kMaxDevices];  // device address of g_noalloc_scratch, per device
+// Device address of g_noalloc_scratch, looked up once per device.  A
+// cudaDeviceReset on that device unloads this library's module there, so
+// the cached address does not survive it: callers that reset a device must
+// not call this entry point on it afterwards.
+void* g_addr[kMaxDevices];
 }  // namespace
 
 }  // namespace utl
@@ -67,9 +70,10 @@ extern "C" int utl_pack_batch_u32_noalloc(uint8_t flag, const uint32_t* d_values
     }
     scratch = g_addr[dev];
   }
-  // The array keeps the previous call's contents; utl_pack_batch_u32
-  // clears the counter and tile states it uses on `stream` before its
-  // kernel runs.
-  return utl_pack_batch_u32(flag, d_values, d_val_off, d_block_start, n_streams, n_blocks, d_out, out_cap,
-                            d_block_off, d_stream_byte_off, scratch, kNoAllocScratchBytes, d_err, stream);
+  // The array keeps the previous call's contents; the pack clears the
+  // counter and tile states it uses on `stream` before its kernel runs.
+  // may_alloc = false: the launch takes no allocating step at all (the
+  // uint32 pack's mapped-memory window hint is skipped).
+  return pack_batch_device(false, false, flag, d_values, d_val_off, d_block_start, n_streams, n_blocks, d_out, out_cap,
+                           d_block_off, d_stream_byte_off, scratch, kNoAllocScratchBytes, d_err, (cudaStream_t)stream);
 }
