@@ -239,18 +239,28 @@ def host_threads():
 
 
 def cpu_round_trip(values_np, val_off, flag, threads, min_seconds=10.0, max_rounds=50, rounds=None):
-    """Pack + unpack the sample with the oracle on `threads` host threads.
-    Returns (list of per-round seconds)."""
+    """Pack + unpack the values on `threads` host threads with the CPU
+    restatement of the reference's vectorized pipelines (AVX-512, else
+    AVX2: oracle/utl_simd.c), into output buffers allocated once (as a
+    caller packing into preallocated slices would).  Returns the per-round
+    seconds."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_ref as O
     times = []
+    out = bo = None
+    vals_out = np.empty_like(values_np)
     t_start = time.perf_counter()
     while True:
         t0 = time.perf_counter()
-        packed, bo, _ = O.pack_streams(flag, values_np, val_off, n_threads=threads)
-        out, err = O.unpack_streams(packed, bo, val_off, dtype=values_np.dtype, n_threads=threads)
+        packed, bo, _ = O.pack_streams(flag, values_np, val_off, n_threads=threads, simd=True, out=out, bo=bo,
+                                       want_so=False)
+        _, err = O.unpack_streams(packed, bo, val_off, dtype=values_np.dtype, n_threads=threads, simd=True,
+                                  out=vals_out)
         t1 = time.perf_counter()
         assert err == 0
+        if out is None:
+            out = packed.base if packed.base is not None else packed
+            assert np.array_equal(vals_out, values_np), "CPU round trip mismatch"
         times.append(t1 - t0)
         if rounds is not None:
             if len(times) >= rounds:
@@ -260,44 +270,100 @@ def cpu_round_trip(values_np, val_off, flag, threads, min_seconds=10.0, max_roun
     return times
 
 
+def cpu_kind():
+    """Which CPU pipeline the baseline times, for the JSON line."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_ref as O
+    lv = O.simd_level()
+    name = {2: "AVX-512", 1: "AVX2"}.get(lv, "scalar")
+    return ("%s restatement of the reference's packBlockAVX512/unpackBlockAVX512 pipelines "
+            "(oracle/utl_simd.c; AVX-512 before AVX2 as the reference dispatches)" % name)
+
+
 def c3_sample_host(n, seed):
     rng = np.random.default_rng(seed)
-    v = rng.integers(0, 256, n, dtype=np.uint64)
-    m = rng.random(n) < 0.02
-    v[m] = rng.integers(256, 2**32, int(m.sum()), dtype=np.uint64)
-    v = v.astype(np.uint32)
+    v = rng.integers(0, 256, n, dtype=np.uint32)
+    m = rng.random(n, dtype=np.float32) < 0.02
+    v[m] = rng.integers(256, 2**32, int(m.sum()), dtype=np.uint64).astype(np.uint32)
     nb = n // 128
     sel = rng.random(nb) < 0.10
-    c = rng.integers(0, 256, nb, dtype=np.uint64).astype(np.uint32)
+    c = rng.integers(0, 256, nb, dtype=np.uint32)
     vb = v.reshape(nb, 128)
     vb[sel] = c[sel][:, None]
     return v
 
 
+def make_workload_host(name, seed, log2n=28):
+    """Host (numpy) version of make_workload: the same shapes and
+    distributions (other random draws), for the CPU reference arm."""
+    rng = np.random.default_rng(seed)
+    if name.startswith("c3"):
+        n = 1 << log2n
+        return c3_sample_host(n, seed), np.array([0, n], dtype=np.uint64)
+    if name == "c1":
+        n = 1 << 20
+        return rng.integers(0, 2**11, n, dtype=np.uint32), np.array([0, n], dtype=np.uint64)
+    if name == "c2":
+        lens = loguniform_lengths(rng, 1000, 128, 2**20)
+        vo = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+        v = np.empty(int(vo[-1]), dtype=np.uint32)
+        for s, ln in enumerate(lens):
+            v[int(vo[s]):int(vo[s + 1])] = np.cumsum(rng.geometric(1 / 64, int(ln)), dtype=np.int64).astype(np.uint32)
+        return v, vo
+    if name == "c4":
+        lens = loguniform_lengths(rng, 512, 128, 2**18).astype(np.float64)
+        lens = np.maximum(128, np.round(lens * (2**26 / lens.sum()))).astype(np.int64)
+        vo = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+        parts = []
+        for s, ln in enumerate(lens):
+            kind = s % 3
+            if kind == 0:
+                x = np.uint64(2**40) + rng.integers(0, 2**20, int(ln), dtype=np.uint64)
+            elif kind == 1:
+                x = rng.integers(0, 2**64 - 1, int(ln), dtype=np.uint64, endpoint=True)
+            else:
+                x = (np.int64(2**62) + np.cumsum(rng.integers(-1000, 1001, int(ln)))).astype(np.uint64)
+            parts.append(x)
+        return np.concatenate(parts), vo
+    raise ValueError(name)
+
+
+def workload_config(name, n, n_blocks, world):
+    """The config object both arms print (the workload, not its packed
+    size, which depends on the random draws)."""
+    wl = WORKLOADS[name]
+    return {"workload": wl["desc"], "flag": wl["flag"], "values_per_gpu": n, "blocks_per_gpu": n_blocks,
+            "l2": "inputs larger than L2 (no flush)" if n * (8 if wl["is64"] else 4) > L2_BYTES else "inputs fit L2",
+            "parallelism": "replicas" if world > 1 else "1 GPU"}
+
+
 # --------------------------------------------------------------------------
 def run_reference(args):
-    """The reference arm: the reference's CPU algorithm (the oracle's plain-C
-    restatement; the Go reference has no toolchain here) on the host cores,
-    same metric and workload shape, each step one bounded sample."""
+    """The reference arm: the reference's CPU algorithm on the host cores
+    (the Go module needs a Go 1.27 toolchain, absent here, so its AVX-512 /
+    AVX2 pipelines run as restated in C), on this arm's workload at full
+    size, all host threads, same metric."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     wl = WORKLOADS[args.workload]
     threads = host_threads()
-    S = 1 << 24
-    vals = c3_sample_host(S, 99)
-    vo = np.array([0, S], dtype=np.uint64)
+    vals, vo = make_workload_host(args.workload, 1234, args.log2n)
+    n = int(vo[-1])
+    esz = vals.dtype.itemsize
+    nb = int(sum((int(vo[s + 1] - vo[s]) + 127) // 128 for s in range(len(vo) - 1)))
     cpu_round_trip(vals, vo, wl["flag"], threads, rounds=max(args.warmup, 1))
     times = cpu_round_trip(vals, vo, wl["flag"], threads, rounds=args.steps)
     t = sum(times) / len(times)
-    gbps = 2 * 4 * S / t / 1e9
-    sample = "%d u32 values (%d MiB) of the workload's distribution per step" % (S, 4 * S >> 20)
+    gbps = 2 * esz * n / t / 1e9
+    sample = "the whole workload (%d values, %d MiB) per step" % (n, esz * n >> 20)
     line = {"metric": "round-trip uncompressed GB/s (batched PackUint32 + UnpackUint32)", "value": gbps,
             "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32", "data": "synthetic (seeded, workload distribution)",
-            "config": {"workload": wl["desc"], "flag": wl["flag"], "sample_values": S},
-            "cpu_baseline": {"value": gbps, "unit": "GB/s", "cores": threads, "kind": "port", "sample": sample},
+            "dtype": "u64" if esz == 8 else "u32", "data": "synthetic (seeded, the workload's distribution, on host)",
+            "config": workload_config(args.workload, n, nb, 1),
+            "cpu_baseline": {"value": gbps, "unit": "GB/s", "cores": threads, "kind": "port", "impl": cpu_kind(),
+                             "sample": sample},
             "e2e": {"value": gbps, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -486,6 +552,7 @@ def main():
     ap.add_argument("--workload", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the per-call drop-in sample")
     ap.add_argument("--no-index", action="store_true", help="skip timing the stream indexer")
     ap.add_argument("--no-get", action="store_true", help="skip timing the batched Get")
     ap.add_argument("--log2n", type=int, default=28, help="values per GPU of the c3 workloads (2^log2n)")
@@ -691,16 +758,55 @@ def main():
                "queries_drawn": "stream uniform among non-empty streams, position uniform in it",
                "timing": "CUDA events, one batched launch per call"}
 
+    # the plain per-call drop-in on the same data: one utl_pack_u32 and one
+    # utl_unpack_u32 call per 128-value block (host buffers), the way a Go
+    # caller would use the per-call API block after block; a bounded sample
+    plain = None
+    if rank == 0 and not args.no_plain and not is64:
+        nblk = min(codec.n_blocks, 2000)
+        hv = values[:nblk * 128].cpu().numpy().view(np.uint32).copy()
+        hv_n = min(hv.size, n)
+        buf = np.zeros(L.utl_max_block_length32(flag), dtype=np.uint8)
+        outb = np.zeros(128, dtype=np.uint32)
+        olen, cnt, cons, ovf = C.c_size_t(0), C.c_int(0), C.c_size_t(0), C.c_int(0)
+        pu8 = buf.ctypes.data_as(C.POINTER(C.c_uint8))
+        pout = outb.ctypes.data_as(C.POINTER(C.c_uint32))
+        lat_p, lat_u = [], []
+        for rep in range(2):  # the first pass warms the per-thread context
+            lat_p.clear()
+            lat_u.clear()
+            for i in range(0, hv_n, 128):
+                blk = hv[i:i + 128]
+                t0 = time.perf_counter()
+                rc = L.utl_pack_u32(flag, blk.ctypes.data_as(C.POINTER(C.c_uint32)), blk.size, pu8, buf.size,
+                                    C.byref(olen))
+                t1 = time.perf_counter()
+                assert rc == 0, rc
+                rc = L.utl_unpack_u32(pu8, olen.value, pout, C.byref(cnt), C.byref(cons), C.byref(ovf))
+                t2 = time.perf_counter()
+                assert rc == 0 and cnt.value == blk.size and np.array_equal(outb[:blk.size], blk)
+                lat_p.append(t1 - t0)
+                lat_u.append(t2 - t1)
+        tot = sum(lat_p) + sum(lat_u)
+        plain = {"GBps": 2 * 4 * hv_n / tot / 1e9, "unit": "GB/s (round-trip uncompressed)", "blocks": hv_n // 128,
+                 "pack_us_p50": 1e6 * float(np.median(lat_p)), "pack_us_p99": 1e6 * float(np.percentile(lat_p, 99)),
+                 "unpack_us_p50": 1e6 * float(np.median(lat_u)),
+                 "unpack_us_p99": 1e6 * float(np.percentile(lat_u, 99)),
+                 "calls": "utl_pack_u32 + utl_unpack_u32 per 128-value block, host buffers, one thread",
+                 "sample": "the workload's first %d blocks" % (hv_n // 128)}
+
     cpu = None
-    if rank == 0 and not args.no_cpu and args.workload.startswith("c3"):
+    if rank == 0 and not args.no_cpu:
+        # the same values, copied to the host, through the CPU restatement
+        # of the reference's vectorized pipelines on every host thread
         threads = host_threads()
-        S = 1 << 24
-        sample = values[:S].cpu().numpy().view(np.uint32).copy()
-        svo = np.array([0, S], dtype=np.uint64)
-        times = cpu_round_trip(sample, svo, flag, threads)
+        host_vals = values.cpu().numpy().view(np.uint64 if is64 else np.uint32)
+        times = cpu_round_trip(host_vals, vo, flag, threads, min_seconds=10.0, max_rounds=10)
+        del host_vals
         t = sum(times) / len(times)
-        cpu = {"value": 2 * 4 * S / t / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
-               "sample": "first %d values (%d MiB) of this workload, %d rounds" % (S, 4 * S >> 20, len(times))}
+        cpu = {"value": 2 * value_bytes / t / 1e9, "unit": "GB/s", "cores": threads, "kind": "port",
+               "impl": cpu_kind(),
+               "sample": "the whole workload (%d values, %d MiB), %d rounds" % (n, value_bytes >> 20, len(times))}
 
     if rank == 0:
         line = {
@@ -708,9 +814,8 @@ def main():
             "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u64" if is64 else "u32", "data": "synthetic (seeded on device)",
-            "config": {"workload": wl["desc"], "flag": flag, "values_per_gpu": n, "blocks_per_gpu": codec.n_blocks,
-                       "packed_bytes_per_gpu": packed_len, "bytes_per_value": packed_len / n,
-                       "l2": "inputs larger than L2 (no flush)", "parallelism": "replicas" if world > 1 else "1 GPU"},
+            "config": workload_config(args.workload, n, codec.n_blocks, world),
+            "packed": {"bytes_per_gpu": packed_len, "bytes_per_value": packed_len / n},
             "pack": {"ms": pack_ms, "uncompressed_GBps": value_bytes / (pack_ms * 1e-3) / 1e9,
                      "hbm_GBps": pack_gbs, "hbm_frac": pack_gbs / peak},
             "unpack": {"ms": unpack_ms, "uncompressed_GBps": value_bytes / (unpack_ms * 1e-3) / 1e9,
@@ -718,6 +823,8 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "plain_per_call": plain,
+            "batched_e2e_over_plain": (e2e["value"] / plain["GBps"]) if (e2e and plain) else None,
             "index": index,
             "get": get,
             "gpu_launches": int(launches),

@@ -19,6 +19,7 @@
  * blocks, never the value returned for a valid block.
  */
 #include "utl_oracle.h"
+#include "utl_oracle_int.h"
 
 #include <pthread.h>
 #include <stdlib.h>
@@ -383,11 +384,7 @@ int utlo_pack_u32(uint8_t flag, const uint32_t *values, int n, uint8_t *dst, siz
 
 /* ---------------- block unpack: unpack_block.go + scalar.go:260-309 ---------------- */
 
-typedef struct {
-  size_t consumed, p_off, block_end;
-  uint32_t for_base;
-  int count, bw, exc, has_exc, delta, zigzag, has_for, u64single, empty;
-} uhdr_t;
+typedef utlo_uhdr_t uhdr_t;
 
 static int check_int_type(int t, int for_u64) {
   if (for_u64) return t == T_U64 ? UTLO_OK : UTLO_ERR_UNSUPPORTED_TYPE; /* header.go:187 */
@@ -531,6 +528,25 @@ int utlo_unpack_u32(const uint8_t *src, size_t src_len, uint32_t *out, int *coun
   *count = n;
   *consumed = c;
   return UTLO_OK;
+}
+
+/* ---------------- shared internals (utl_oracle_int.h) ---------------- */
+
+const utlo_block_impl utlo_scalar_impl = {pack_block, unpack_block};
+
+uint32_t utlo_i_encode_header(int count, int bw, int exc, uint32_t flags) { return encode_header(count, bw, exc, flags); }
+int utlo_i_estimate_exc_cost(int exc, int step_delta) { return estimate_exc_cost(exc, step_delta); }
+int utlo_i_select_for_width(uint32_t m) { return select_for_width(m); }
+int utlo_i_delta_encode(uint32_t *v, int n) { return delta_encode(v, n); }
+void utlo_i_delta_decode(uint32_t *v, int n, int use_zz) { delta_decode(v, n, use_zz); }
+int utlo_i_delta_decode_overflow(uint32_t *v, int n) { return delta_decode_overflow(v, n); }
+int utlo_i_svb_encode(uint8_t *dst, const uint32_t *v, int n) { return svb_encode(dst, v, n); }
+int utlo_i_decode_unpack_header(const uint8_t *buf, size_t len, int for_u64, utlo_uhdr_t *o) {
+  return decode_unpack_header(buf, len, for_u64, o);
+}
+int utlo_i_apply_exceptions(uint32_t *dst, const uint8_t *buf, size_t len, size_t exc_start, int count, int bw,
+                            int exc, size_t *consumed) {
+  return apply_exceptions(dst, buf, len, exc_start, count, bw, exc, consumed);
 }
 
 /* ---------------- Get: get.go ---------------- */
@@ -743,7 +759,8 @@ int utlo_max_block_length64(uint8_t flag) { return 2 * utlo_max_block_length32(f
 /* ---------------- uint64: uint64.go ---------------- */
 
 /* uint64.go:302-333 with packFor64 (:147) and packUint64TwoBlock (:161) */
-int utlo_pack_u64(uint8_t flag, const uint64_t *v, int n, uint8_t *dst, size_t *out_len) {
+int utlo_i_pack_u64(const utlo_block_impl *im, uint8_t flag, const uint64_t *v, int n, uint8_t *dst,
+                    size_t *out_len) {
   if (n <= 0 || n > BLOCK) return UTLO_ERR_INVALID_BUFFER;
   uint8_t inner = (uint8_t)(flag & ~UTLO_APPEND);
   uint64_t mn = v[0], mx = v[0], acc = 0;
@@ -754,7 +771,7 @@ int utlo_pack_u64(uint8_t flag, const uint64_t *v, int n, uint8_t *dst, size_t *
   if (!(inner & UTLO_NOFOR) && mn > 0 && (mx - mn) < (1ull << 32)) {
     for (int i = 0; i < n; i++) lo[i] = (uint32_t)(v[i] - mn);
     size_t ilen;
-    err = pack_block((uint8_t)(inner | UTLO_NOFOR), lo, n, dst + FOR64_BASE, t64, 0, &ilen);
+    err = im->pack((uint8_t)(inner | UTLO_NOFOR), lo, n, dst + FOR64_BASE, t64, 0, &ilen);
     if (err) return err;
     /* uint64.go:124-142: move header(+svbLen) forward, insert the base */
     uint32_t hw = ld32(dst + FOR64_BASE);
@@ -767,13 +784,13 @@ int utlo_pack_u64(uint8_t flag, const uint64_t *v, int n, uint8_t *dst, size_t *
   }
   if ((acc >> 32) == 0) {
     for (int i = 0; i < n; i++) lo[i] = (uint32_t)v[i];
-    return pack_block(inner, lo, n, dst, t64, 0, out_len);
+    return im->pack(inner, lo, n, dst, t64, 0, out_len);
   }
   for (int i = 0; i < n; i++) { lo[i] = (uint32_t)v[i]; hi[i] = (uint32_t)(v[i] >> 32); }
   size_t l1, l2;
-  err = pack_block(inner, lo, n, dst, t64 | H_COMBINE, 1, &l1);
+  err = im->pack(inner, lo, n, dst, t64 | H_COMBINE, 1, &l1);
   if (err) return err;
-  err = pack_block(inner, hi, n, dst + l1, t64, 0, &l2);
+  err = im->pack(inner, hi, n, dst + l1, t64, 0, &l2);
   if (err) return err;
   hdr_t h1 = decode_header(ld32(dst));
   st16(dst + HDR + (h1.has_exc ? SVBLEN_BYTES : 0) + for_base_bytes(h1.forw), (uint32_t)l2);
@@ -781,8 +798,13 @@ int utlo_pack_u64(uint8_t flag, const uint64_t *v, int n, uint8_t *dst, size_t *
   return UTLO_OK;
 }
 
+int utlo_pack_u64(uint8_t flag, const uint64_t *v, int n, uint8_t *dst, size_t *out_len) {
+  return utlo_i_pack_u64(&utlo_scalar_impl, flag, v, n, dst, out_len);
+}
+
 /* uint64.go:191-266 */
-int utlo_unpack_u64(const uint8_t *buf, size_t len, uint64_t *out, int *count, size_t *consumed, int *ovf) {
+int utlo_i_unpack_u64(const utlo_block_impl *im, const uint8_t *buf, size_t len, uint64_t *out, int *count,
+                      size_t *consumed, int *ovf) {
   if (len < HDR) return UTLO_ERR_INVALID_BUFFER;
   hdr_t h = decode_header(ld32(buf));
   if (h.int_type != T_U64) return UTLO_ERR_UNSUPPORTED_TYPE;
@@ -797,27 +819,31 @@ int utlo_unpack_u64(const uint8_t *buf, size_t len, uint64_t *out, int *count, s
       if (len < off + FOR64_BASE) return UTLO_ERR_INVALID_BUFFER;
       base = ld64(buf + off);
     }
-    err = unpack_block(buf, len, 1, lo, &n, &c1, ovf, NULL);
+    err = im->unpack(buf, len, 1, lo, &n, &c1, ovf, NULL);
     if (err) return err;
     for (int i = 0; i < n; i++) out[i] = (uint64_t)lo[i] + base;
     *count = n;
     *consumed = c1;
     return UTLO_OK;
   }
-  err = unpack_block(buf, len, 1, lo, &n, &c1, ovf, NULL);
+  err = im->unpack(buf, len, 1, lo, &n, &c1, ovf, NULL);
   if (err) return err;
   int forb = for_base_bytes(h.forw);
   size_t meta = HDR + (h.has_exc ? SVBLEN_BYTES : 0) + (size_t)forb + B2LEN_BYTES;
   if (len < meta) return UTLO_ERR_INVALID_BUFFER;
   size_t b2len = ld16(buf + meta - B2LEN_BYTES);
   if (c1 + b2len > len) return UTLO_ERR_INVALID_BUFFER;
-  err = unpack_block(buf + c1, b2len, 1, hi, &n2, &c2, ovf, NULL);
+  err = im->unpack(buf + c1, b2len, 1, hi, &n2, &c2, ovf, NULL);
   if (err) return err;
   if (n2 != n) return UTLO_ERR_INVALID_BUFFER;
   for (int i = 0; i < n; i++) out[i] = ((uint64_t)hi[i] << 32) | lo[i];
   *count = n;
   *consumed = c1 + b2len;
   return UTLO_OK;
+}
+
+int utlo_unpack_u64(const uint8_t *buf, size_t len, uint64_t *out, int *count, size_t *consumed, int *ovf) {
+  return utlo_i_unpack_u64(&utlo_scalar_impl, buf, len, out, count, consumed, ovf);
 }
 
 /* uint64.go:372-436 */
@@ -859,6 +885,7 @@ int utlo_get_u64(int pos, const uint8_t *buf, size_t len, uint64_t *value, int *
 static int64_t n_blocks_of(uint64_t n) { return (int64_t)((n + BLOCK - 1) / BLOCK); }
 
 typedef struct {
+  const utlo_block_impl *im;
   int is64;
   uint8_t flag;
   const void *values;
@@ -870,6 +897,7 @@ typedef struct {
   size_t used;
   uint32_t *lens;        /* per-block lengths, b1-b0 */
   int err;
+  struct pack_shared *shared;
 } pack_job_t;
 
 static int stream_of_block(const int64_t *bstart, int n_streams, int64_t b) {
@@ -881,21 +909,52 @@ static int stream_of_block(const int64_t *bstart, int n_streams, int64_t b) {
   return lo;
 }
 
+/* Shared state of one pack_streams call: each worker packs its block range
+ * into its own buffer, waits for all, then copies its bytes to their final
+ * place and writes its blocks' offsets (both phases run in parallel). */
+typedef struct pack_shared {
+  pthread_barrier_t bar;
+  pack_job_t *jobs;
+  int n_threads;
+  uint8_t *out;
+  size_t out_cap;
+  uint64_t *block_off;
+  int64_t nb;
+} pack_shared_t;
+
 static void *pack_worker(void *arg) {
   pack_job_t *j = (pack_job_t *)arg;
-  if (j->b0 >= j->b1) return NULL;
-  int s = stream_of_block(j->bstart, j->n_streams, j->b0);
-  for (int64_t b = j->b0; b < j->b1; b++) {
-    while (b >= j->bstart[s + 1]) s++;
-    uint64_t first = j->val_off[s] + (uint64_t)(b - j->bstart[s]) * BLOCK;
-    uint64_t last = j->val_off[s + 1];
-    int n = (int)((last - first) < BLOCK ? (last - first) : BLOCK);
-    size_t l = 0;
-    int err = j->is64 ? utlo_pack_u64(j->flag, (const uint64_t *)j->values + first, n, j->buf + j->used, &l)
-                      : utlo_pack_u32(j->flag, (const uint32_t *)j->values + first, n, j->buf + j->used, &l);
-    if (err) { j->err = err; return NULL; }
-    j->lens[b - j->b0] = (uint32_t)l;
-    j->used += l;
+  if (j->b0 < j->b1) {
+    int s = stream_of_block(j->bstart, j->n_streams, j->b0);
+    for (int64_t b = j->b0; b < j->b1; b++) {
+      while (b >= j->bstart[s + 1]) s++;
+      uint64_t first = j->val_off[s] + (uint64_t)(b - j->bstart[s]) * BLOCK;
+      uint64_t last = j->val_off[s + 1];
+      int n = (int)((last - first) < BLOCK ? (last - first) : BLOCK);
+      size_t l = 0;
+      int err = j->is64 ? utlo_i_pack_u64(j->im, j->flag, (const uint64_t *)j->values + first, n, j->buf + j->used, &l)
+                        : j->im->pack(j->flag, (const uint32_t *)j->values + first, n, j->buf + j->used,
+                                      (uint32_t)T_U32 << H_TYPE_SHIFT, 0, &l);
+      if (err) { j->err = err; break; }
+      j->lens[b - j->b0] = (uint32_t)l;
+      j->used += l;
+    }
+  }
+  pack_shared_t *sh = j->shared;
+  pthread_barrier_wait(&sh->bar);
+  size_t off = 0, total = 0;
+  int err = 0;
+  for (int t = 0; t < sh->n_threads; t++) {
+    if (sh->jobs[t].err) err = 1;
+    if (&sh->jobs[t] < j) off += sh->jobs[t].used;
+    total += sh->jobs[t].used;
+  }
+  if (err || total > sh->out_cap) return NULL;
+  memcpy(sh->out + off, j->buf, j->used);
+  if (sh->block_off) {
+    uint64_t acc = off;
+    for (int64_t b = j->b0; b < j->b1; b++) { sh->block_off[b] = acc; acc += j->lens[b - j->b0]; }
+    if (j->b1 == sh->nb) sh->block_off[sh->nb] = acc;
   }
   return NULL;
 }
@@ -920,10 +979,18 @@ size_t utlo_stream_pack_bound_u64(uint8_t flag, const uint64_t *val_off, int n_s
   return stream_pack_bound(flag, val_off, n_streams, 1);
 }
 
-static int pack_streams(int is64, uint8_t flag, const void *values, const uint64_t *val_off, int n_streams,
-                        uint8_t *out, size_t out_cap, uint64_t *block_off, uint64_t *stream_byte_off,
-                        int n_threads) {
+/* Per-thread output buffers kept from call to call (grown on demand), so
+ * that a timed call does not pay for fresh pages. */
+#define MAX_WS 1024
+static pthread_mutex_t g_ws_mu = PTHREAD_MUTEX_INITIALIZER;
+static uint8_t *g_ws_buf[MAX_WS];
+static size_t g_ws_cap[MAX_WS];
+
+int utlo_i_pack_streams(const utlo_block_impl *im, int is64, uint8_t flag, const void *values,
+                        const uint64_t *val_off, int n_streams, uint8_t *out, size_t out_cap, uint64_t *block_off,
+                        uint64_t *stream_byte_off, int n_threads) {
   if (n_threads < 1) n_threads = 1;
+  if (n_threads > MAX_WS) n_threads = MAX_WS;
   int64_t *bs = block_starts(val_off, n_streams);
   int64_t nb = bs[n_streams];
   pack_job_t *jobs = (pack_job_t *)calloc((size_t)n_threads, sizeof(pack_job_t));
@@ -931,51 +998,63 @@ static int pack_streams(int is64, uint8_t flag, const void *values, const uint64
   size_t maxb = (size_t)(is64 ? utlo_max_block_length64(flag) : utlo_max_block_length32(flag));
   uint32_t *lens = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(nb > 0 ? nb : 1));
   int err = UTLO_OK;
+  pack_shared_t sh;
+  sh.jobs = jobs; sh.n_threads = n_threads; sh.out = out; sh.out_cap = out_cap; sh.block_off = block_off; sh.nb = nb;
+  pthread_barrier_init(&sh.bar, NULL, (unsigned)n_threads);
+  pthread_mutex_lock(&g_ws_mu);
   for (int t = 0; t < n_threads; t++) {
     pack_job_t *j = &jobs[t];
-    j->is64 = is64; j->flag = flag; j->values = values; j->val_off = val_off; j->bstart = bs;
+    j->im = im; j->is64 = is64; j->flag = flag; j->values = values; j->val_off = val_off; j->bstart = bs;
     j->n_streams = n_streams;
     j->b0 = nb * t / n_threads; j->b1 = nb * (t + 1) / n_threads;
-    j->buf = (uint8_t *)malloc(maxb * (size_t)(j->b1 - j->b0) + 1);
+    const size_t need = maxb * (size_t)(j->b1 - j->b0) + 1;
+    if (g_ws_cap[t] < need) {
+      free(g_ws_buf[t]);
+      g_ws_buf[t] = (uint8_t *)malloc(need);
+      g_ws_cap[t] = g_ws_buf[t] ? need : 0;
+    }
+    j->buf = g_ws_buf[t];
     j->lens = lens + j->b0;
+    j->shared = &sh;
+    if (!j->buf) err = UTLO_ERR_INVALID_BUFFER;
   }
-  for (int t = 1; t < n_threads; t++) pthread_create(&th[t], NULL, pack_worker, &jobs[t]);
-  pack_worker(&jobs[0]);
-  for (int t = 1; t < n_threads; t++) pthread_join(th[t], NULL);
-  size_t total = 0;
-  for (int t = 0; t < n_threads; t++) { if (jobs[t].err && !err) err = jobs[t].err; total += jobs[t].used; }
-  if (!err && total > out_cap) err = UTLO_ERR_INVALID_BUFFER;
   if (!err) {
-    size_t off = 0;
-    for (int t = 0; t < n_threads; t++) { memcpy(out + off, jobs[t].buf, jobs[t].used); off += jobs[t].used; }
-    uint64_t acc = 0;
-    for (int64_t b = 0; b < nb; b++) { if (block_off) block_off[b] = acc; acc += lens[b]; }
-    if (block_off) block_off[nb] = acc;
-    if (stream_byte_off) {
-      /* stream s starts where its first block does */
-      uint64_t a = 0;
-      int64_t b = 0;
-      for (int s = 0; s <= n_streams; s++) {
-        while (b < bs[s]) a += lens[b++];
-        stream_byte_off[s] = a;
-      }
+    for (int t = 1; t < n_threads; t++) pthread_create(&th[t], NULL, pack_worker, &jobs[t]);
+    pack_worker(&jobs[0]);
+    for (int t = 1; t < n_threads; t++) pthread_join(th[t], NULL);
+    size_t total = 0;
+    for (int t = 0; t < n_threads; t++) { if (jobs[t].err && !err) err = jobs[t].err; total += jobs[t].used; }
+    if (!err && total > out_cap) err = UTLO_ERR_INVALID_BUFFER;
+  }
+  pthread_mutex_unlock(&g_ws_mu);
+  if (!err && block_off && nb == 0) block_off[0] = 0;
+  if (!err && stream_byte_off) {
+    /* stream s starts where its first block does */
+    uint64_t a = 0;
+    int64_t b = 0;
+    for (int s = 0; s <= n_streams; s++) {
+      while (b < bs[s]) a += lens[b++];
+      stream_byte_off[s] = a;
     }
   }
-  for (int t = 0; t < n_threads; t++) free(jobs[t].buf);
+  pthread_barrier_destroy(&sh.bar);
   free(jobs); free(th); free(lens); free(bs);
   return err;
 }
 
 int utlo_pack_streams_u32(uint8_t flag, const uint32_t *values, const uint64_t *val_off, int n_streams, uint8_t *out,
                           size_t out_cap, uint64_t *block_off, uint64_t *stream_byte_off, int n_threads) {
-  return pack_streams(0, flag, values, val_off, n_streams, out, out_cap, block_off, stream_byte_off, n_threads);
+  return utlo_i_pack_streams(&utlo_scalar_impl, 0, flag, values, val_off, n_streams, out, out_cap, block_off,
+                             stream_byte_off, n_threads);
 }
 int utlo_pack_streams_u64(uint8_t flag, const uint64_t *values, const uint64_t *val_off, int n_streams, uint8_t *out,
                           size_t out_cap, uint64_t *block_off, uint64_t *stream_byte_off, int n_threads) {
-  return pack_streams(1, flag, values, val_off, n_streams, out, out_cap, block_off, stream_byte_off, n_threads);
+  return utlo_i_pack_streams(&utlo_scalar_impl, 1, flag, values, val_off, n_streams, out, out_cap, block_off,
+                             stream_byte_off, n_threads);
 }
 
 typedef struct {
+  const utlo_block_impl *im;
   int is64;
   const uint8_t *packed;
   const uint64_t *block_off, *val_off;
@@ -1001,16 +1080,24 @@ static void *unpack_worker(void *arg) {
     size_t off = j->block_off[b], blen = j->block_off[b + 1] - off;
     int n = 0, ovf = 0;
     size_t c = 0;
-    int err = j->is64 ? utlo_unpack_u64(j->packed + off, blen, (uint64_t *)j->values + first, &n, &c, &ovf)
-                      : utlo_unpack_u32(j->packed + off, blen, (uint32_t *)j->values + first, &n, &c, &ovf);
+    int err;
+    if (j->is64) {
+      err = utlo_i_unpack_u64(j->im, j->packed + off, blen, (uint64_t *)j->values + first, &n, &c, &ovf);
+    } else if (want == BLOCK) {
+      err = j->im->unpack(j->packed + off, blen, 0, (uint32_t *)j->values + first, &n, &c, &ovf, NULL);
+    } else {
+      uint32_t tmp[BLOCK];
+      err = j->im->unpack(j->packed + off, blen, 0, tmp, &n, &c, &ovf, NULL);
+      if (!err && n == want) memcpy((uint32_t *)j->values + first, tmp, (size_t)n * 4);
+    }
     if (!err && (n != want || c != blen)) err = UTLO_ERR_INVALID_BUFFER;
     if (err) { j->err = err; return NULL; }
   }
   return NULL;
 }
 
-static int unpack_streams(int is64, const uint8_t *packed, const uint64_t *block_off, const uint64_t *val_off,
-                          int n_streams, void *values, int n_threads) {
+int utlo_i_unpack_streams(const utlo_block_impl *im, int is64, const uint8_t *packed, const uint64_t *block_off,
+                          const uint64_t *val_off, int n_streams, void *values, int n_threads) {
   if (n_threads < 1) n_threads = 1;
   int64_t *bs = block_starts(val_off, n_streams);
   int64_t nb = bs[n_streams];
@@ -1018,7 +1105,7 @@ static int unpack_streams(int is64, const uint8_t *packed, const uint64_t *block
   pthread_t *th = (pthread_t *)calloc((size_t)n_threads, sizeof(pthread_t));
   for (int t = 0; t < n_threads; t++) {
     unpack_job_t *j = &jobs[t];
-    j->is64 = is64; j->packed = packed; j->block_off = block_off; j->val_off = val_off; j->bstart = bs;
+    j->im = im; j->is64 = is64; j->packed = packed; j->block_off = block_off; j->val_off = val_off; j->bstart = bs;
     j->n_streams = n_streams; j->values = values;
     j->b0 = nb * t / n_threads; j->b1 = nb * (t + 1) / n_threads;
   }
@@ -1033,11 +1120,11 @@ static int unpack_streams(int is64, const uint8_t *packed, const uint64_t *block
 
 int utlo_unpack_streams_u32(const uint8_t *packed, const uint64_t *block_off, const uint64_t *val_off, int n_streams,
                             uint32_t *values, int n_threads) {
-  return unpack_streams(0, packed, block_off, val_off, n_streams, values, n_threads);
+  return utlo_i_unpack_streams(&utlo_scalar_impl, 0, packed, block_off, val_off, n_streams, values, n_threads);
 }
 int utlo_unpack_streams_u64(const uint8_t *packed, const uint64_t *block_off, const uint64_t *val_off, int n_streams,
                             uint64_t *values, int n_threads) {
-  return unpack_streams(1, packed, block_off, val_off, n_streams, values, n_threads);
+  return utlo_i_unpack_streams(&utlo_scalar_impl, 1, packed, block_off, val_off, n_streams, values, n_threads);
 }
 
 /* Batched Get over packed streams: the block index of stream s's first

@@ -112,6 +112,29 @@ void utlo_get_streams_u64(const uint8_t *packed, const uint64_t *block_off, cons
                           const uint32_t *q_stream, const uint64_t *q_pos, int64_t n_queries, uint64_t *out,
                           int32_t *status);
 
+/* The reference's vectorized pipelines (utl_simd.c): AVX-512 when the CPU
+ * has it, else AVX2, else the scalar path.  Same contracts and bytes as
+ * the functions above.  utlo_simd_set_level lowers the level for tests
+ * (2 AVX-512, 1 AVX2, 0 scalar) and returns the level in force. */
+int utlo_simd_level(void);
+int utlo_simd_set_level(int level);
+int utlo_simd_pack_u32(uint8_t flag, const uint32_t *values, int n, uint8_t *dst, size_t *out_len);
+int utlo_simd_unpack_u32(const uint8_t *src, size_t src_len, uint32_t *out, int *count, size_t *consumed,
+                         int *ovf_pos);
+int utlo_simd_pack_u64(uint8_t flag, const uint64_t *values, int n, uint8_t *dst, size_t *out_len);
+int utlo_simd_unpack_u64(const uint8_t *src, size_t src_len, uint64_t *out, int *count, size_t *consumed,
+                         int *ovf_pos);
+int utlo_simd_pack_streams_u32(uint8_t flag, const uint32_t *values, const uint64_t *val_off, int n_streams,
+                               uint8_t *out, size_t out_cap, uint64_t *block_off, uint64_t *stream_byte_off,
+                               int n_threads);
+int utlo_simd_pack_streams_u64(uint8_t flag, const uint64_t *values, const uint64_t *val_off, int n_streams,
+                               uint8_t *out, size_t out_cap, uint64_t *block_off, uint64_t *stream_byte_off,
+                               int n_threads);
+int utlo_simd_unpack_streams_u32(const uint8_t *packed, const uint64_t *block_off, const uint64_t *val_off,
+                                 int n_streams, uint32_t *values, int n_threads);
+int utlo_simd_unpack_streams_u64(const uint8_t *packed, const uint64_t *block_off, const uint64_t *val_off,
+                                 int n_streams, uint64_t *values, int n_threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,8 +23,9 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        src = os.path.join(ODIR, "utl_oracle.c")
-        if not os.path.exists(SO) or os.path.getmtime(SO) < os.path.getmtime(src):
+        srcs = [os.path.join(ODIR, f) for f in ("utl_oracle.c", "utl_simd.c", "utl_simd_body.inc", "utl_oracle.h",
+                                                 "utl_oracle_int.h", "Makefile")]
+        if not os.path.exists(SO) or any(os.path.getmtime(SO) < os.path.getmtime(f) for f in srcs):
             subprocess.check_call(["make", "-s", "-C", ODIR])
         L = C.CDLL(SO)
         P8, PU32, PU64, SZ = C.POINTER(C.c_uint8), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_size_t)
@@ -47,6 +48,19 @@ def lib():
         L.utlo_pack_streams_u64.argtypes = [C.c_uint8, PU64, PU64, C.c_int, P8, C.c_size_t, PU64, PU64, C.c_int]
         L.utlo_unpack_streams_u32.argtypes = [P8, PU64, PU64, C.c_int, PU32, C.c_int]
         L.utlo_unpack_streams_u64.argtypes = [P8, PU64, PU64, C.c_int, PU64, C.c_int]
+        for pre in ("utlo_simd_",):
+            getattr(L, pre + "pack_u32").argtypes = [C.c_uint8, PU32, C.c_int, P8, SZ]
+            getattr(L, pre + "pack_u64").argtypes = [C.c_uint8, PU64, C.c_int, P8, SZ]
+            getattr(L, pre + "unpack_u32").argtypes = [P8, C.c_size_t, PU32, PI, SZ, PI]
+            getattr(L, pre + "unpack_u64").argtypes = [P8, C.c_size_t, PU64, PI, SZ, PI]
+            getattr(L, pre + "pack_streams_u32").argtypes = [C.c_uint8, PU32, PU64, C.c_int, P8, C.c_size_t, PU64,
+                                                             PU64, C.c_int]
+            getattr(L, pre + "pack_streams_u64").argtypes = [C.c_uint8, PU64, PU64, C.c_int, P8, C.c_size_t, PU64,
+                                                             PU64, C.c_int]
+            getattr(L, pre + "unpack_streams_u32").argtypes = [P8, PU64, PU64, C.c_int, PU32, C.c_int]
+            getattr(L, pre + "unpack_streams_u64").argtypes = [P8, PU64, PU64, C.c_int, PU64, C.c_int]
+        L.utlo_simd_level.argtypes = []
+        L.utlo_simd_set_level.argtypes = [C.c_int]
         PI32 = C.POINTER(C.c_int32)
         L.utlo_get_streams_u32.argtypes = [P8, PU64, PU64, C.c_int, PU32, PU64, C.c_int64, PU32, PI32]
         L.utlo_get_streams_u32.restype = None
@@ -67,37 +81,49 @@ def _bytes(src):
     return b
 
 
-def pack_u32(flag, values):
+def _fn(name, simd):
+    return getattr(lib(), ("utlo_simd_" if simd else "utlo_") + name)
+
+
+def simd_level(level=None):
+    """The vectorized pipelines' level (2 AVX-512, 1 AVX2, 0 scalar); with
+    an argument, lower it first (None: leave it)."""
+    if level is not None:
+        return lib().utlo_simd_set_level(level)
+    return lib().utlo_simd_level()
+
+
+def pack_u32(flag, values, simd=False):
     v = np.ascontiguousarray(values, dtype=np.uint32)
     dst = np.zeros(2048, dtype=np.uint8)
     n = C.c_size_t(0)
-    err = lib().utlo_pack_u32(flag, _p(v, C.c_uint32), len(v), _p(dst, C.c_uint8), C.byref(n))
+    err = _fn("pack_u32", simd)(flag, _p(v, C.c_uint32), len(v), _p(dst, C.c_uint8), C.byref(n))
     return (bytes(dst[:n.value]) if err == 0 else None), err
 
 
-def pack_u64(flag, values):
+def pack_u64(flag, values, simd=False):
     v = np.ascontiguousarray(values, dtype=np.uint64)
     dst = np.zeros(4096, dtype=np.uint8)
     n = C.c_size_t(0)
-    err = lib().utlo_pack_u64(flag, _p(v, C.c_uint64), len(v), _p(dst, C.c_uint8), C.byref(n))
+    err = _fn("pack_u64", simd)(flag, _p(v, C.c_uint64), len(v), _p(dst, C.c_uint8), C.byref(n))
     return (bytes(dst[:n.value]) if err == 0 else None), err
 
 
-def unpack_u32(src):
+def unpack_u32(src, simd=False):
     b = _bytes(src)
     out = np.zeros(128, dtype=np.uint32)
     cnt, cons, ovf = C.c_int(0), C.c_size_t(0), C.c_int(0)
-    err = lib().utlo_unpack_u32(_p(b, C.c_uint8), len(b), _p(out, C.c_uint32), C.byref(cnt), C.byref(cons), C.byref(ovf))
+    err = _fn("unpack_u32", simd)(_p(b, C.c_uint8), len(b), _p(out, C.c_uint32), C.byref(cnt), C.byref(cons), C.byref(ovf))
     if err:
         return None, 0, err, ovf.value
     return out[:cnt.value].copy(), cons.value, 0, 0
 
 
-def unpack_u64(src):
+def unpack_u64(src, simd=False):
     b = _bytes(src)
     out = np.zeros(128, dtype=np.uint64)
     cnt, cons, ovf = C.c_int(0), C.c_size_t(0), C.c_int(0)
-    err = lib().utlo_unpack_u64(_p(b, C.c_uint8), len(b), _p(out, C.c_uint64), C.byref(cnt), C.byref(cons), C.byref(ovf))
+    err = _fn("unpack_u64", simd)(_p(b, C.c_uint8), len(b), _p(out, C.c_uint64), C.byref(cnt), C.byref(cons), C.byref(ovf))
     if err:
         return None, 0, err, ovf.value
     return out[:cnt.value].copy(), cons.value, 0, 0
@@ -139,40 +165,46 @@ def max_block_length64(flag):
     return lib().utlo_max_block_length64(flag)
 
 
-def pack_streams(flag, values, val_off, n_threads=4):
-    """Returns (packed bytes ndarray, block_off, stream_byte_off)."""
+def pack_streams(flag, values, val_off, n_threads=4, simd=False, out=None, bo=None, want_so=True):
+    """Returns (packed bytes ndarray, block_off, stream_byte_off).  simd:
+    through the vectorized pipelines (the same bytes).  out / bo: buffers
+    to reuse (capacity at least the stream bound / n_blocks + 1)."""
     is64 = values.dtype == np.uint64
     L = lib()
     vo = np.ascontiguousarray(val_off, dtype=np.uint64)
     ns = len(vo) - 1
     bound_fn = L.utlo_stream_pack_bound_u64 if is64 else L.utlo_stream_pack_bound_u32
     cap = bound_fn(flag, _p(vo, C.c_uint64), ns)
-    out = np.zeros(max(cap, 1), dtype=np.uint8)
-    nb = int(sum((int(vo[s + 1] - vo[s]) + 127) // 128 for s in range(ns)))
-    bo = np.zeros(nb + 1, dtype=np.uint64)
-    so = np.zeros(ns + 1, dtype=np.uint64)
+    if out is None or out.size < cap:
+        out = np.empty(max(cap, 1), dtype=np.uint8)
+    nb = int(np.sum((vo[1:] - vo[:-1] + np.uint64(127)) // np.uint64(128))) if ns else 0
+    if bo is None or bo.size < nb + 1:
+        bo = np.zeros(nb + 1, dtype=np.uint64)
+    so = np.zeros(ns + 1, dtype=np.uint64) if want_so else None
+    pso = _p(so, C.c_uint64) if want_so else None
     if is64:
-        err = L.utlo_pack_streams_u64(flag, _p(values, C.c_uint64), _p(vo, C.c_uint64), ns, _p(out, C.c_uint8), cap,
-                                      _p(bo, C.c_uint64), _p(so, C.c_uint64), n_threads)
+        err = _fn("pack_streams_u64", simd)(flag, _p(values, C.c_uint64), _p(vo, C.c_uint64), ns, _p(out, C.c_uint8),
+                                            cap, _p(bo, C.c_uint64), pso, n_threads)
     else:
-        err = L.utlo_pack_streams_u32(flag, _p(values, C.c_uint32), _p(vo, C.c_uint64), ns, _p(out, C.c_uint8), cap,
-                                      _p(bo, C.c_uint64), _p(so, C.c_uint64), n_threads)
+        err = _fn("pack_streams_u32", simd)(flag, _p(values, C.c_uint32), _p(vo, C.c_uint64), ns, _p(out, C.c_uint8),
+                                            cap, _p(bo, C.c_uint64), pso, n_threads)
     assert err == 0, err
-    return out[:int(bo[-1])], bo, so
+    return out[:int(bo[nb])], bo[:nb + 1], so
 
 
-def unpack_streams(packed, block_off, val_off, dtype=np.uint32, n_threads=4):
+def unpack_streams(packed, block_off, val_off, dtype=np.uint32, n_threads=4, simd=False, out=None):
     L = lib()
     vo = np.ascontiguousarray(val_off, dtype=np.uint64)
     bo = np.ascontiguousarray(block_off, dtype=np.uint64)
     pk = np.ascontiguousarray(packed, dtype=np.uint8)
-    out = np.zeros(int(vo[-1]), dtype=dtype)
+    if out is None:
+        out = np.zeros(int(vo[-1]), dtype=dtype)
     if dtype == np.uint64:
-        err = L.utlo_unpack_streams_u64(_p(pk, C.c_uint8), _p(bo, C.c_uint64), _p(vo, C.c_uint64), len(vo) - 1,
-                                        _p(out, C.c_uint64), n_threads)
+        err = _fn("unpack_streams_u64", simd)(_p(pk, C.c_uint8), _p(bo, C.c_uint64), _p(vo, C.c_uint64), len(vo) - 1,
+                                              _p(out, C.c_uint64), n_threads)
     else:
-        err = L.utlo_unpack_streams_u32(_p(pk, C.c_uint8), _p(bo, C.c_uint64), _p(vo, C.c_uint64), len(vo) - 1,
-                                        _p(out, C.c_uint32), n_threads)
+        err = _fn("unpack_streams_u32", simd)(_p(pk, C.c_uint8), _p(bo, C.c_uint64), _p(vo, C.c_uint64), len(vo) - 1,
+                                              _p(out, C.c_uint32), n_threads)
     return out, err
 
 
