@@ -276,11 +276,16 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
 /* Process-wide knobs of the batched kernels, set by the autotuner
  * (utlpfor_b200.tune); no counterpart in the reference.  Defaults are
  * sound on any B200.
- *   UTL_KNOB_UNPACK_SCHEDULE: 0 = one CTA per 32 blocks; 2 = persistent
- *     warps with the next group's bytes in flight (cp.async double buffer),
- *     staging up to 528 bytes a block; 3 = the same staging up to 264 bytes
- *     a block (more warps resident); 1 = 3 or 2 by the batch's mean block
- *     length, decided on the device (the default).
+ *   UTL_KNOB_UNPACK_SCHEDULE: the uint32 unpack kernel.  0 = one CTA per
+ *     32 blocks; 2 = persistent warps with the next group's bytes in
+ *     flight (cp.async double buffer), staging up to 528 bytes a block;
+ *     3 = the same staging up to 264 bytes a block (more warps resident);
+ *     1 = 3 or 2 by the batch's mean block length, decided on the device;
+ *     5 = persistent warps staging each group of 8 blocks with one TMA bulk
+ *     copy, three groups in flight, up to 264 bytes a block, with the
+ *     register fast path for blocks of at most 16 exceptions; 6 = the same
+ *     with two groups of up to 528 bytes a block in flight; 4 = 5 or 6 by
+ *     the batch's mean block length, decided on the device (the default).
  *   UTL_KNOB_PACK_CTAS_PER_SM: cap on resident pack CTAs per SM (0 = the
  *     occupancy maximum).
  *   UTL_KNOB_PACK_SCHEDULE: uint32 pack kernel, 0 = four threads per block

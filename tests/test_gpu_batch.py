@@ -27,8 +27,11 @@ def to_dev(torch, a):
 LENS = [1, 128, 300, 0, 257, 1000, 5, 129, 0, 4096, 77]
 
 
-@pytest.fixture(params=[0, 1, 2, 3], ids=["unpack_tiles", "unpack_pipelined", "unpack_pipelined_wide",
-                                          "unpack_pipelined_narrow"])
+UNPACK_SCHEDULES = {0: "unpack_tiles", 1: "unpack_pipelined", 2: "unpack_pipelined_wide",
+                    3: "unpack_pipelined_narrow", 4: "unpack_tma", 5: "unpack_tma_narrow", 6: "unpack_tma_wide"}
+
+
+@pytest.fixture(params=sorted(UNPACK_SCHEDULES), ids=[UNPACK_SCHEDULES[k] for k in sorted(UNPACK_SCHEDULES)])
 def sched(request):
     from utlpfor_b200._lib import load
     L = load()
@@ -53,10 +56,11 @@ KINDS = ["small", "exc", "dense_exc", "sorted", "walk", "wide", "const", "zero",
 
 @pytest.mark.parametrize("flag", list(range(16)))
 @pytest.mark.parametrize("kind", KINDS)
-def test_pack_unpack_batch_u32(env, flag, kind, sched, psched):
+def test_pack_unpack_batch_u32(env, flag, kind, psched):
     """Every combination of the four stored flag bits (Delta, NoFOR,
-    NoPatch, Special) under every pack and unpack schedule."""
-    _batch_u32_case(env, flag, kind)
+    NoPatch, Special) under every pack schedule, each result unpacked
+    under every unpack schedule."""
+    _batch_u32_case(env, flag, kind, all_unpack=True)
 
 
 @pytest.mark.parametrize("flag", [f | extra for extra in (16, 32, 48) for f in range(16)])
@@ -67,7 +71,7 @@ def test_pack_unpack_batch_u32_placement_flags(env, flag, kind, psched):
     _batch_u32_case(env, flag, kind)
 
 
-def _batch_u32_case(env, flag, kind):
+def _batch_u32_case(env, flag, kind, all_unpack=False):
     U, torch = env
     rng = np.random.default_rng(flag * 31 + len(kind))
     vals, vo = streams(rng, LENS, kind)
@@ -78,8 +82,16 @@ def _batch_u32_case(env, flag, kind):
     assert np.array_equal(pb.packed[:got_len].cpu().numpy(), want)
     assert np.array_equal(pb.block_off.cpu().numpy().view(np.uint64), wbo)
     assert np.array_equal(pb.stream_byte_off.cpu().numpy().view(np.uint64), wso)
-    out = U.unpack_batch(pb)
-    assert np.array_equal(out.cpu().numpy().view(np.uint32), vals)
+    from utlpfor_b200._lib import load
+    L = load()
+    old = L.utl_get_knob(0)
+    try:
+        for sc in (sorted(UNPACK_SCHEDULES) if all_unpack else [old]):
+            assert L.utl_set_knob(0, sc) == 0
+            out = U.unpack_batch(pb)
+            assert np.array_equal(out.cpu().numpy().view(np.uint32), vals), UNPACK_SCHEDULES[sc]
+    finally:
+        L.utl_set_knob(0, old)
 
 
 @pytest.mark.parametrize("flag", list(range(16)) + [16 | 5, 32 | 9, 48 | 15])

@@ -523,6 +523,7 @@ static int unpack_batch(bool u64, const uint8_t* d_packed, size_t packed_len, co
   a.values = d_values;
   a.block_status = d_status;
   a.err = d_err;
+  a.spin_limit = launch::spin_limit();
   cudaError_t e = launch::unpack(u64, a, st);
   return e == cudaSuccess ? UTL_OK : cuda_fail(e);
 }

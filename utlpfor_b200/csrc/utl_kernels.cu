@@ -22,6 +22,7 @@
 #include "utl_launch.h"
 #include "utl_lane.cuh"
 #include "utl_quad.cuh"
+#include "utl_unpack.cuh"
 
 namespace utl {
 
@@ -776,6 +777,222 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackAr
     nxt = nn;
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// TMA-staged pipelined unpack (utl_unpack.cuh): persistent warps over
+// groups of 8 blocks, NSTAGE groups in flight per warp, each group's bytes
+// brought in by one bulk copy on its stage's mbarrier.
+template <int STAGE, int NSTAGE>
+struct QuadTmaSmem {
+  uint4 stage[kQWarps][NSTAGE][(STAGE + kQStagePad) / 16];
+  uint4 patch[kQWarps][8][kBlock / 4 + 1];  // +16 B: quads start on different banks
+  uint64_t bar[kQWarps][NSTAGE];
+};
+
+// Offsets of group g for the TMA pipeline: lane l <= nb holds
+// block_off[8g + l]; lane 0 also the stream of block 8g (in `s0`).
+struct TmaGroup {
+  uint64_t off;
+  int s0;
+};
+__device__ __forceinline__ TmaGroup tma_group_load(const UnpackArgs& a, int64_t g, int lane) {
+  TmaGroup t;
+  const int64_t b0 = g * 8;
+  const int nb = b0 < a.n_blocks ? (int)min((int64_t)8, a.n_blocks - b0) : 0;
+  t.off = (nb > 0 && lane <= nb) ? a.block_off[b0 + lane] : 0ull;
+  t.s0 = (nb > 0 && lane == 0) ? stream_of(a.block_start, a.n_streams, b0) : 0;
+  return t;
+}
+__device__ __forceinline__ int tma_group_nb(const UnpackArgs& a, int64_t g) {
+  const int64_t b0 = g * 8;
+  return b0 < a.n_blocks ? (int)min((int64_t)8, a.n_blocks - b0) : 0;
+}
+template <int STAGE>
+__device__ __forceinline__ bool tma_group_fits(const UnpackArgs& a, const TmaGroup& t, int nb, int lane) {
+  if (nb <= 0) return false;
+  GroupInfo gi;
+  gi.off = t.off;
+  gi.b0 = 0;
+  gi.nb = nb;
+  gi.s0 = 0;
+  return group_fits<STAGE>(a, gi, lane);
+}
+
+// Copy the 16-byte chunks [c0, c1) of the aligned range starting at a0 (the
+// chunks of buf's ends that the bulk copy leaves out) with plain loads;
+// bytes outside the buffer read as zero.
+__device__ __forceinline__ void stage_edge(uint4* dst16, uintptr_t a0, uintptr_t lo, uintptr_t hi, int c0, int c1,
+                                           int lane) {
+  for (int c = c0 + lane; c < c1; c += 32) {
+    const uintptr_t a = a0 + 16 * (uintptr_t)c;
+    uint32_t w[4] = {0, 0, 0, 0};
+    for (int bb = 0; bb < 16; bb++) {
+      const uintptr_t x = a + bb;
+      if (x >= lo && x < hi) w[bb >> 2] |= (uint32_t)(*(const uint8_t*)x) << ((bb & 3) * 8);
+    }
+    dst16[c] = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+// Put group gi (which fits the stage) in flight into dst: one bulk copy of
+// the buffer's aligned interior part, plain loads for the edge chunks.
+// Returns whether a bulk copy was issued (then bar completes with it).
+__device__ __forceinline__ bool stage_issue(const UnpackArgs& a, const TmaGroup& gi, int nb, uint4* dst16,
+                                            uint64_t* bar, int lane) {
+  const uint64_t o0 = __shfl_sync(kFull, gi.off, 0), o1 = __shfl_sync(kFull, gi.off, nb);
+  const uintptr_t lo = (uintptr_t)a.packed, hi = lo + a.packed_len;
+  const uintptr_t a0 = (lo + o0) & ~(uintptr_t)15, a1 = (lo + o1 + 15) & ~(uintptr_t)15;
+  const uintptr_t lo16 = (lo + 15) & ~(uintptr_t)15, hi16 = hi & ~(uintptr_t)15;
+  const uintptr_t t0 = a0 > lo16 ? a0 : lo16, t1 = a1 < hi16 ? a1 : hi16;
+  const int nch = (int)((a1 - a0) >> 4);
+  if (t1 > t0) {
+    if (lane == 0) {
+      tma::proxy_fence();
+      tma::mbar_expect_tx(bar, (uint32_t)(t1 - t0));
+      tma::bulk_load((uint8_t*)dst16 + (t0 - a0), (const void*)t0, (uint32_t)(t1 - t0), bar);
+    }
+    const int c0 = (int)((t0 - a0) >> 4), c1 = (int)((t1 - a0) >> 4);
+    if (c0 > 0) stage_edge(dst16, a0, lo, hi, 0, c0, lane);
+    if (c1 < nch) stage_edge(dst16, a0, lo, hi, c1, nch, lane);
+    return true;
+  }
+  stage_edge(dst16, a0, lo, hi, 0, nch, lane);
+  return false;
+}
+
+template <int STAGE, int NSTAGE, bool AUTO>
+__global__ void __launch_bounds__(kQThreads, 5) unpack_quad_tma_kernel(UnpackArgs a) {
+  extern __shared__ uint4 smem4[];
+  QuadTmaSmem<STAGE, NSTAGE>& S = *(QuadTmaSmem<STAGE, NSTAGE>*)smem4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (AUTO) {
+    const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
+    const bool wide = span > kWideMean * (uint64_t)a.n_blocks;
+    if (wide != (STAGE == kPStageWide)) return;
+  }
+  const int q = lane >> 2, j = lane & 3;
+  const unsigned qm = quad::quad_mask(lane);
+  const int64_t n_groups = (a.n_blocks + 7) / 8;
+  const int64_t stride = (int64_t)gridDim.x * kQWarps;
+  int64_t g = (int64_t)blockIdx.x * kQWarps + warp;
+  if (g >= n_groups) return;
+  uint32_t* patch = (uint32_t*)S.patch[warp][q];
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s < NSTAGE; s++) tma::mbar_init(&S.bar[warp][s], 1);
+    tma::mbar_init_fence();
+  }
+  __syncwarp();
+  const uint32_t lim = a.spin_limit;
+  uint32_t pend = 0, phase = 0, fits = 0;  // per stage slot: copy in flight, parity of its next completion; per group: fits
+
+  // groups in flight: gq[0] is the current group (stage st), gq[k] the
+  // k-th after it
+  TmaGroup gq[NSTAGE];
+#pragma unroll
+  for (int k = 0; k < NSTAGE; k++) {
+    gq[k] = tma_group_load(a, g + k * stride, lane);
+    if (tma_group_fits<STAGE>(a, gq[k], tma_group_nb(a, g + k * stride), lane)) fits |= 1u << k;
+  }
+#pragma unroll
+  for (int k = 0; k < NSTAGE - 1; k++)
+    if (((fits >> k) & 1u) && stage_issue(a, gq[k], tma_group_nb(a, g + k * stride), S.stage[warp][k],
+                                          &S.bar[warp][k], lane))
+      pend |= 1u << k;
+  bool timed_out = false;
+  int st = 0;  // stage of the current group
+  for (; g < n_groups; g += stride) {
+    // the group NSTAGE-1 ahead goes in flight into the stage freed last round
+    const int sn = st == 0 ? NSTAGE - 1 : st - 1;
+    if (((fits >> (NSTAGE - 1)) & 1u) &&
+        stage_issue(a, gq[NSTAGE - 1], tma_group_nb(a, g + (NSTAGE - 1) * stride), S.stage[warp][sn],
+                    &S.bar[warp][sn], lane))
+      pend |= 1u << sn;
+    if ((pend >> st) & 1u) {
+      if (!tma::mbar_wait(&S.bar[warp][st], (phase >> st) & 1u, lim)) {
+        timed_out = true;
+        break;
+      }
+      pend &= ~(1u << st);
+      phase ^= 1u << st;
+    }
+    __syncwarp();
+
+    const int nb = tma_group_nb(a, g);
+    const bool cur_fits = fits & 1u;
+    const uint64_t off0 = __shfl_sync(kFull, gq[0].off, 0);
+    const uint64_t s = __shfl_sync(kFull, gq[0].off, q), e = __shfl_sync(kFull, gq[0].off, q + 1);
+    const bool bad = e < s || e - s > (uint64_t)kMaxBlock32 || e > a.packed_len;
+    const int64_t b = g * 8 + q;
+    const int s0 = __shfl_sync(kFull, gq[0].s0, 0);
+    const int rounds = cur_fits ? 1 : nb;
+    uint4* stg = S.stage[warp][st];
+#pragma unroll 1
+    for (int rd = 0; rd < rounds; rd++) {
+      if (!cur_fits) {
+        // one block per round, synchronously, through this group's buffer
+        const uint64_t rs = __shfl_sync(kFull, gq[0].off, rd), re = __shfl_sync(kFull, gq[0].off, rd + 1);
+        __syncwarp();
+        if (re >= rs && re - rs <= (uint64_t)kMaxBlock32 && re <= a.packed_len)
+          stage_bytes(stg, a.packed, a.packed_len, rs, re, lane, 32);
+        __syncwarp();
+      }
+      if (cur_fits ? q < nb : q == rd) {
+        uint64_t first;
+        int want;
+        span_in(a.val_off, a.block_start, stream_from(a.block_start, a.n_streams, s0, b), b, &first, &want);
+        int status = kOK, ovf = 0;
+        if (bad) {
+          status = kErrCountMismatch;
+        } else {
+          const int len = (int)(e - s);
+          const int blk = cur_fits ? (int)(((uintptr_t)a.packed + off0) & 15) + (int)(s - off0)
+                                   : (int)(((uintptr_t)a.packed + s) & 15);
+          uint32_t* op = (uint32_t*)a.values + first;
+          const SmemBytes sb{(const uint32_t*)stg};
+          quad::QFast f;
+          uint32_t x[8][4];
+          quad::QResult r;
+          if (quad::fast_plan(sb, blk, len, j, qm, f)) r = quad::fast_decode(sb, blk, f, x, patch, j, qm);
+          else r = quad::quad_unpack_block(sb, blk, len, false, x, patch, j, qm);
+          status = r.status;
+          ovf = r.ovf;
+          if (status == kOK && (r.count != want || r.consumed != len)) status = kErrCountMismatch;
+          if (status == kOK) {
+            if (want == kBlock) {
+              quad::quad_store_full(op, x, patch, j, qm);
+            } else {
+#pragma unroll
+              for (int v = 0; v < 8; v++)
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                  if (16 * v + 4 * j + k < want) op[16 * v + 4 * j + k] = x[v][k];
+            }
+          }
+        }
+        if (j == 0) {
+          if (a.block_status) a.block_status[b] = status | (ovf << 8);
+          if (status != kOK && a.err) atomicOr(a.err, 1u << status);
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < NSTAGE - 1; k++) gq[k] = gq[k + 1];
+    fits >>= 1;
+    gq[NSTAGE - 1] = tma_group_load(a, g + NSTAGE * stride, lane);
+    if (tma_group_fits<STAGE>(a, gq[NSTAGE - 1], tma_group_nb(a, g + NSTAGE * stride), lane))
+      fits |= 1u << (NSTAGE - 1);
+    st = st == NSTAGE - 1 ? 0 : st + 1;
+  }
+  if (timed_out) {
+    // record it, then let every copy still in flight land (bounded) before
+    // the warp leaves
+    if (lane == 0 && a.err) atomicOr(a.err, 1u << 10);
+#pragma unroll
+    for (int s2 = 0; s2 < NSTAGE; s2++)
+      if ((pend >> s2) & 1u) tma::mbar_wait(&S.bar[warp][s2], (phase >> s2) & 1u, lim);
+  }
 }
 
 struct QuadPackSmem {
@@ -1756,6 +1973,8 @@ struct DevCfg {
   int quad_pack_ctas = 0;        // pack_quad_kernel
   int pipe_ctas = 0;             // unpack_quad_pipe_kernel, narrow staging
   int pipe_wide_ctas = 0;        // unpack_quad_pipe_kernel, wide staging
+  int tma_ctas = 0;              // unpack_quad_tma_kernel, narrow staging (3 stages)
+  int tma_wide_ctas = 0;         // unpack_quad_tma_kernel, wide staging (2 stages)
   int pack_ctas[2] = {0, 0};     // pack_kernel<false/true>
   // Mapped pinned pair the uint32 lane pack's last block fills with the
   // batch's packed bytes and block count; the next allocating launch on
@@ -1863,8 +2082,19 @@ static cudaError_t unpack_pipe(const UnpackArgs& a, cudaStream_t st, int ctas) {
   note_launch(1);
   return cudaGetLastError();
 }
-// 0: one CTA per 32 blocks; 1: persistent pipelined warps (selectable for tuning)
-static int g_unpack_schedule = 1;
+template <int STAGE, int NSTAGE, bool AUTO>
+static cudaError_t unpack_tma(const UnpackArgs& a, cudaStream_t st, int ctas) {
+  const size_t smem = sizeof(QuadTmaSmem<STAGE, NSTAGE>);
+  const int64_t groups = (a.n_blocks + 7) / 8;
+  int64_t grid = (int64_t)num_sms() * ctas;
+  const int64_t need = (groups + kQWarps - 1) / kQWarps;
+  if (grid > need) grid = need;
+  unpack_quad_tma_kernel<STAGE, NSTAGE, AUTO><<<(unsigned)grid, kQThreads, smem, st>>>(a);
+  note_launch(1);
+  return cudaGetLastError();
+}
+// UTL_KNOB_UNPACK_SCHEDULE (include/utlpfor.h)
+static int g_unpack_schedule = 4;
 static int g_pack_cap = 0;
 static int g_pack_schedule = 1;
 // Test knobs: the polls of every bounded wait (0 = the default 2^22), and
@@ -1911,6 +2141,13 @@ static cudaError_t setup_device(int dev, DevCfg& c) {
   if ((e = set_smem(unpack_quad_pipe_kernel<kPStageWide, false>, pw)) != cudaSuccess) return e;
   c.pipe_ctas = occupancy(unpack_quad_pipe_kernel<kPStageNarrow, false>, kQThreads, pn);
   c.pipe_wide_ctas = occupancy(unpack_quad_pipe_kernel<kPStageWide, false>, kQThreads, pw);
+  const size_t tn = sizeof(QuadTmaSmem<kPStageNarrow, 3>), tw = sizeof(QuadTmaSmem<kPStageWide, 2>);
+  if ((e = set_smem(unpack_quad_tma_kernel<kPStageNarrow, 3, true>, tn)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_tma_kernel<kPStageNarrow, 3, false>, tn)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_tma_kernel<kPStageWide, 2, true>, tw)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_tma_kernel<kPStageWide, 2, false>, tw)) != cudaSuccess) return e;
+  c.tma_ctas = occupancy(unpack_quad_tma_kernel<kPStageNarrow, 3, false>, kQThreads, tn);
+  c.tma_wide_ctas = occupancy(unpack_quad_tma_kernel<kPStageWide, 2, false>, kQThreads, tw);
   if ((e = set_smem(unpack_kernel<false>, unpack_smem(false))) != cudaSuccess) return e;
   if ((e = set_smem(unpack_kernel<true>, unpack_smem(true))) != cudaSuccess) return e;
   return cudaSuccess;
@@ -1982,6 +2219,13 @@ cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
       if (e != cudaSuccess) return e;
       return unpack_pipe<kPStageWide, true>(a, st, c->pipe_wide_ctas);
     }
+    if (g_unpack_schedule == 4) {  // TMA staging, by the batch's mean block length on the device
+      e = unpack_tma<kPStageNarrow, 3, true>(a, st, c->tma_ctas);
+      if (e != cudaSuccess) return e;
+      return unpack_tma<kPStageWide, 2, true>(a, st, c->tma_wide_ctas);
+    }
+    if (g_unpack_schedule == 5) return unpack_tma<kPStageNarrow, 3, false>(a, st, c->tma_ctas);
+    if (g_unpack_schedule == 6) return unpack_tma<kPStageWide, 2, false>(a, st, c->tma_wide_ctas);
     if (g_unpack_schedule == 2) return unpack_pipe<kPStageWide, false>(a, st, c->pipe_wide_ctas);
     if (g_unpack_schedule == 3) return unpack_pipe<kPStageNarrow, false>(a, st, c->pipe_ctas);
     const int64_t grid = (a.n_blocks + kQTile - 1) / kQTile;
@@ -2030,7 +2274,7 @@ cudaError_t plain_get(bool u64, int pos, const uint8_t* src, int64_t staged, int
 int set_knob(int knob, int value) {
   switch (knob) {
     case 0:  // UTL_KNOB_UNPACK_SCHEDULE
-      if (value < 0 || value > 3) return -1;
+      if (value < 0 || value > 6) return -1;
       g_unpack_schedule = value;
       return 0;
     case 1:  // UTL_KNOB_PACK_CTAS_PER_SM (0 = occupancy maximum)

@@ -34,6 +34,7 @@ struct UnpackArgs {
   void* values;
   int32_t* block_status;
   uint32_t* err;
+  uint32_t spin_limit = 1u << 22;  // polls of each bounded wait (UTL_KNOB_SPIN_LIMIT)
 };
 
 struct GetArgs {
