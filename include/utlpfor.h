@@ -289,7 +289,14 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *   UTL_KNOB_PACK_CTAS_PER_SM: cap on resident pack CTAs per SM (0 = the
  *     occupancy maximum).
  *   UTL_KNOB_PACK_SCHEDULE: uint32 pack kernel, 0 = four threads per block
- *     (CTA tiles), 1 = one thread per block (independent warp tiles).
+ *     (CTA tiles), 1 = one thread per block (independent warp tiles of 32
+ *     blocks), 2 = a lane pair per block (independent warp tiles of 16
+ *     blocks, half the shared memory per warp, more warps per SM).
+ *   UTL_KNOB_PACK_WINDOW: the tile image of the one-thread and lane-pair
+ *     packs, 0 = by the block density of the previous pack on this device
+ *     that may allocate (a hint read without waiting), 1 = the large window,
+ *     2 = the small window (for batches of at most about 144 bytes a block).
+ *     Outputs are the same for every value.
  *   UTL_KNOB_HOST_PIPELINE: the host-buffer batch calls, 0 = one pass
  *     (all copies in, kernels, all copies out); 1 = batches of 64 MiB of
  *     values or more are cut at block boundaries into pieces of
@@ -310,6 +317,7 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
 #define UTL_KNOB_HOST_PIPELINE 3
 #define UTL_KNOB_SPIN_LIMIT 4
 #define UTL_KNOB_KEEP_SCRATCH 5
+#define UTL_KNOB_PACK_WINDOW 6
 UTL_API int utl_set_knob(int knob, int value);
 UTL_API int utl_get_knob(int knob);
 

@@ -41,7 +41,7 @@ def sched(request):
     L.utl_set_knob(0, old)
 
 
-@pytest.fixture(params=[0, 1], ids=["pack_quad", "pack_lane"])
+@pytest.fixture(params=[0, 1, 2], ids=["pack_quad", "pack_lane", "pack_pair"])
 def psched(request):
     from utlpfor_b200._lib import load
     L = load()

@@ -23,6 +23,7 @@
 #include "utl_lane.cuh"
 #include "utl_quad.cuh"
 #include "utl_unpack.cuh"
+#include "utl_pair.cuh"
 
 namespace utl {
 
@@ -1671,6 +1672,191 @@ __global__ void __launch_bounds__(kLThreads, 8) pack_lane_kernel(PackArgs a) {
 }
 
 // ------------------------------------------------------------------------
+// Pack, a lane pair per block (utl_pair.cuh): the lane pack's loop over
+// tiles of 16 blocks.  Each warp works alone: take a tile, load it (16-byte
+// cp.async into 544-byte slots), plan every block (a pair per block), scan
+// the lengths and publish the tile's aggregate at once; write the blocks
+// into the warp's image while the window loads of the tile's offset are in
+// flight; take, load, plan and publish the next tile; then stream the image
+// out at the resolved offset.
+// ------------------------------------------------------------------------
+template <int SHAPE>
+struct PairWarpSmem {
+  uint4 in[16 * pair::kSlot / 16];
+  uint4 img[pair::Window<SHAPE>::kImageBytes / 16];
+};
+static_assert(pair::kSlot % 16 == 0, "16-byte slots");
+
+// Issue the loads of tile `tile` (16 blocks) into the slots; returns this
+// lane's block value count (0 past the last block); shift as for the lane
+// pack (whole tiles one contiguous run 1..3 words past a 16-byte boundary).
+__device__ __noinline__ void pair_issue_shifted(uint8_t* inb, const uint8_t* src, int lane) {
+  for (int c = lane; c < 16 * 33; c += 32) {
+    const int k = c / 33, q = c - 33 * k;
+    cp_async16(inb + k * pair::kSlot + 16 * q, src + 512 * k + 16 * q);
+  }
+}
+__device__ __forceinline__ int pair_load_tile(const PackArgs& a, int64_t tile, uint8_t* inb, int lane, int& shift) {
+  const int kb = lane >> 1;
+  const int64_t gb = tile * 16 + kb;
+  uint64_t first = 0;
+  int n = 0;
+  shift = 0;
+  const int s0 = __shfl_sync(kFull, lane == 0 ? stream_of(a.block_start, a.n_streams, tile * 16) : 0, 0);
+  if (gb < a.n_blocks) span_in(a.val_off, a.block_start, stream_from(a.block_start, a.n_streams, s0, gb), gb, &first, &n);
+  const uint32_t* vals = (const uint32_t*)a.values;
+  const uint64_t f0 = __shfl_sync(kFull, first, 0);
+  const bool whole = __all_sync(kFull, n == kBlock && first == f0 + (uint64_t)kBlock * kb);
+  const int mis = (int)(((uintptr_t)(vals + f0) >> 2) & 3);
+  if (whole && mis == 0) {
+    const uint8_t* src = (const uint8_t*)(vals + f0) + 16 * lane;
+    uint8_t* dst = inb + 16 * lane;
+#pragma unroll 8
+    for (int k = 0; k < 16; k++) {
+      cp_async16(dst + k * pair::kSlot, src + 512 * k);
+      cp_async16(dst + k * pair::kSlot + 256, src + 512 * k + 256);
+    }
+  } else if (whole && (((uintptr_t)vals) & 15) == 0 && f0 - (uint64_t)mis >= a.val_off[0] &&
+             f0 - (uint64_t)mis + 16 * kBlock + 4 <= a.val_off[a.n_streams]) {
+    pair_issue_shifted(inb, (const uint8_t*)(vals + f0 - mis), lane);
+    shift = mis;
+  } else {
+    for (int k = 0; k < 16; k++) {
+      const uint64_t fk = __shfl_sync(kFull, first, 2 * k);
+      const int nk = __shfl_sync(kFull, n, 2 * k);
+      const uint32_t* blk = vals + fk;
+      // 32 chunks of the block: lane l takes chunk l
+      uint8_t* d = inb + k * pair::kSlot + 16 * lane;
+      const uint32_t* sp = blk + 4 * lane;
+      if (nk == kBlock && (((uintptr_t)blk) & 15) == 0) {
+        cp_async16(d, sp);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          if (4 * lane + q < nk) cp_async4(d + 4 * q, sp + q);
+          else *(uint32_t*)(d + 4 * q) = 0u;
+        }
+      }
+    }
+  }
+  cp_async_commit();
+  return n;
+}
+
+template <bool DELTA>
+__device__ __forceinline__ void pair_take_and_plan(const PackArgs& a, const LaneScan& sc, uint8_t* inb, uint4* slot,
+                                                   int lane, unsigned pm, int64_t& t, int& n, lane::Plan& p,
+                                                   int& incl, int& total) {
+  unsigned long long tv = 0;
+  if (lane == 0) tv = atomicAdd((unsigned long long*)a.counter, 1ull);
+  t = (int64_t)__shfl_sync(kFull, tv, 0);
+  if (t >= a.n_tiles) return;
+  p.len = 0;
+  p.exc = 0;
+  int shift;
+  n = pair_load_tile(a, t, inb, lane, shift);
+  cp_async_wait0();
+  __syncwarp();
+  const int h = lane & 1;
+  if (shift) pair::realign_slot(slot, shift, h, pm);  // warp-uniform
+  if (n > 0) p = pair::plan_block<DELTA>(slot, n, a.flag, h, pm);
+  incl = warp_incl_scan(h == 0 ? p.len : 0, lane);
+  total = __shfl_sync(kFull, incl, 31);
+  if (lane == 31) lane_publish(sc, t, (uint32_t)total);
+}
+
+template <bool DELTA>
+__device__ __forceinline__ void pair_write(const lane::Plan& p, const uint4* slot, uint8_t* o, int h, unsigned pm) {
+  if (__any_sync(__activemask(), p.exc > 0)) pair::write_block<DELTA, true>(p, slot, o, h, pm);
+  else pair::write_block<DELTA, false>(p, slot, o, h, pm);
+}
+
+__device__ __forceinline__ void pair_block_offsets(const PackArgs& a, int64_t tile, int lane, int n, int off,
+                                                   int incl, uint64_t G) {
+  const int64_t gb = tile * 16 + (lane >> 1);
+  if (!(lane & 1) && n > 0) {
+    a.block_off[gb] = G + (uint64_t)off;
+    if (gb == a.n_blocks - 1) {
+      a.block_off[a.n_blocks] = G + (uint64_t)incl;
+      if (a.stats) {  // the batch's packed bytes and blocks, for the next launch's shape
+        a.stats[0] = G + (uint64_t)incl;
+        a.stats[1] = (uint64_t)a.n_blocks;
+      }
+    }
+  }
+}
+
+template <bool DELTA, int SHAPE>
+__global__ void __launch_bounds__(32, SHAPE == 1 ? 18 : 16) pack_pair_kernel(PackArgs a) {
+  extern __shared__ uint4 smem4[];
+  constexpr int kW = pair::Window<SHAPE>::kBytes;
+  const int lane = threadIdx.x & 31;
+  const int h = lane & 1;
+  const unsigned pm = pair::pair_mask(lane);
+  PairWarpSmem<SHAPE>& W = *(PairWarpSmem<SHAPE>*)smem4;
+  uint8_t* inb = (uint8_t*)W.in;
+  uint8_t* img = (uint8_t*)W.img;
+  uint4* slot = (uint4*)(inb + (lane >> 1) * pair::kSlot);
+  LaneScan sc;
+  sc.agg = (uint32_t*)a.tile_status;
+  sc.grp = sc.agg + a.n_tiles;
+  sc.lim = a.spin_limit;
+  int64_t prev = -1;       // the last tile this warp finished
+  uint64_t prev_incl = 0;  // its inclusive prefix
+  int64_t cur = -1;        // the current tile (planned and published)
+  int n = 0, incl = 0, total = 0, n_rounds = 0;
+  lane::Plan p;
+  p.len = 0;
+  LaneWin win;
+  for (;;) {
+    const int off = incl - p.len;
+    if (cur >= 0) {
+      lane_win_issue(sc, prev, cur, lane, win);
+      if (n_rounds <= 1) {
+        if (n > 0) pair_write<DELTA>(p, slot, img + off, h, pm);
+      } else {
+        // a tile larger than the image: its offset first, then one window
+        // of blocks at a time is written and streamed out
+        const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
+        const bool fits = G + (uint64_t)total <= a.out_cap;
+        if (!fits && lane == 0 && a.err) atomicOr(a.err, 1u << 9);
+        const int my_round = n > 0 ? off / kW : -1;
+        for (int r = 0; r < n_rounds; r++) {
+          const unsigned in_r = __ballot_sync(kFull, my_round == r);
+          const unsigned in_next = __ballot_sync(kFull, my_round == r + 1);
+          const int base = __shfl_sync(kFull, off, __ffs(in_r) - 1);
+          const int end = in_next ? __shfl_sync(kFull, off, __ffs(in_next) - 1) : total;
+          if (my_round == r) pair_write<DELTA>(p, slot, img + (off - base), h, pm);
+          __syncwarp();
+          if (fits) lane_copy_out(W.img, end - base, a.out, G + (uint64_t)base, lane);
+          __syncwarp();
+        }
+        pair_block_offsets(a, cur, lane, n, off, incl, G);
+        prev = cur;
+        prev_incl = G + (uint64_t)total;
+      }
+      __syncwarp();
+    }
+    const int64_t done = cur;
+    const int d_n = n, d_off = off, d_incl = incl, d_total = total, d_rounds = n_rounds;
+    pair_take_and_plan<DELTA>(a, sc, inb, slot, lane, pm, cur, n, p, incl, total);
+    if (done >= 0 && d_rounds <= 1) {
+      const uint64_t G = prev_incl + lane_win_finish(sc, win, lane, a.err);
+      if (G + (uint64_t)d_total <= a.out_cap) lane_copy_out(W.img, d_total, a.out, G, lane);
+      else if (lane == 0 && a.err) atomicOr(a.err, 1u << 9);
+      pair_block_offsets(a, done, lane, d_n, d_off, d_incl, G);
+      prev = done;
+      prev_incl = G + (uint64_t)d_total;
+      __syncwarp();
+    }
+    if (cur >= a.n_tiles) break;
+    const unsigned act = __ballot_sync(kFull, n > 0);
+    const int last = act ? 31 - __clz(act) : 0;
+    n_rounds = act ? __shfl_sync(kFull, incl - p.len, last) / kW + 1 : 0;
+  }
+}
+
+// ------------------------------------------------------------------------
 // Get: one thread per query; queries that need the reference's full-block
 // fallback (delta blocks, deep positions) are resolved by the whole warp.
 // ------------------------------------------------------------------------
@@ -1970,6 +2156,7 @@ struct DevCfg {
   cudaError_t err = cudaSuccess;
   int sms = 0;
   int lane_ctas[3] = {0, 0, 0};  // pack_lane_kernel, per window shape
+  int pair_ctas[2] = {0, 0};     // pack_pair_kernel, per window shape
   int quad_pack_ctas = 0;        // pack_quad_kernel
   int pipe_ctas = 0;             // unpack_quad_pipe_kernel, narrow staging
   int pipe_wide_ctas = 0;        // unpack_quad_pipe_kernel, wide staging
@@ -2100,6 +2287,9 @@ static int g_pack_schedule = 1;
 // Test knobs: the polls of every bounded wait (0 = the default 2^22), and
 // whether the pack leaves the caller's scratch as it finds it.
 static std::atomic<uint32_t> g_spin_limit{0};
+// UTL_KNOB_PACK_WINDOW: 0 = by the previous allocating uint32 pack on this
+// device, 1 = the large image window, 2 = the small one.
+static std::atomic<int> g_pack_window{0};
 static std::atomic<int> g_keep_scratch{0};
 uint32_t spin_limit() {
   const uint32_t v = g_spin_limit.load(std::memory_order_relaxed);
@@ -2127,6 +2317,13 @@ static cudaError_t setup_device(int dev, DevCfg& c) {
   c.lane_ctas[0] = occupancy(pack_lane_kernel<false, 0>, kLThreads, lsm[0]);
   c.lane_ctas[1] = occupancy(pack_lane_kernel<false, 1>, kLThreads, lsm[1]);
   c.lane_ctas[2] = occupancy(pack_lane_kernel<false, 2>, kLThreads, lsm[2]);
+  const size_t psm[2] = {sizeof(PairWarpSmem<0>), sizeof(PairWarpSmem<1>)};
+  if ((e = set_smem(pack_pair_kernel<false, 0>, psm[0])) != cudaSuccess) return e;
+  if ((e = set_smem(pack_pair_kernel<true, 0>, psm[0])) != cudaSuccess) return e;
+  if ((e = set_smem(pack_pair_kernel<false, 1>, psm[1])) != cudaSuccess) return e;
+  if ((e = set_smem(pack_pair_kernel<true, 1>, psm[1])) != cudaSuccess) return e;
+  c.pair_ctas[0] = occupancy(pack_pair_kernel<false, 0>, 32, psm[0]);
+  c.pair_ctas[1] = occupancy(pack_pair_kernel<false, 1>, 32, psm[1]);
   if ((e = set_smem(pack_quad_kernel, sizeof(QuadPackSmem))) != cudaSuccess) return e;
   c.quad_pack_ctas = occupancy(pack_quad_kernel, kQThreads, sizeof(QuadPackSmem));
   if ((e = set_smem(pack_kernel<false>, pack_smem(false))) != cudaSuccess) return e;
@@ -2153,21 +2350,48 @@ static cudaError_t setup_device(int dev, DevCfg& c) {
   return cudaSuccess;
 }
 
+// Window shape of a uint32 pack (0 large, 1 small): the knob, or the block
+// density of the previous allocating pack on this device, read from the
+// mapped pair without waiting (a performance hint only).  Sets a.stats for
+// the kernel to record this batch's density (allocating calls only).
+static int pick_window(PackArgs& a, bool may_alloc, DevCfg& c, uint64_t small_block) {
+  a.stats = may_alloc ? lane_stats_dev(c) : nullptr;
+  const int kn = g_pack_window.load(std::memory_order_relaxed);
+  if (kn == 1) return 0;
+  if (kn == 2) return 1;
+  if (!a.stats) return 0;
+  const volatile uint64_t* hv = c.stats.load(std::memory_order_acquire);
+  const uint64_t bytes = hv[0], blocks = hv[1];
+  return (blocks > 0 && bytes <= blocks * small_block) ? 1 : 0;
+}
+
+template <bool DELTA, int SHAPE>
+static void launch_pair(const PackArgs& a, int64_t grid, cudaStream_t st) {
+  pack_pair_kernel<DELTA, SHAPE><<<(unsigned)grid, 32, sizeof(PairWarpSmem<SHAPE>), st>>>(a);
+}
+
+static cudaError_t pack_pair(const PackArgs& a_in, cudaStream_t st, bool may_alloc, DevCfg& c) {
+  PackArgs a = a_in;
+  a.n_tiles = (a.n_blocks + 15) / 16;
+  const int shape = pick_window(a, may_alloc, c, (uint64_t)pair::kSmallBlock);
+  const int occ = c.pair_ctas[shape];
+  const int per_sm = (g_pack_cap > 0 && g_pack_cap < occ) ? g_pack_cap : occ;
+  int64_t grid = (int64_t)c.sms * per_sm;
+  if (grid > a.n_tiles) grid = a.n_tiles;
+  if (grid < 1) grid = 1;
+  const bool d = (a.flag & kDelta) != 0;
+  if (shape == 1) d ? launch_pair<true, 1>(a, grid, st) : launch_pair<false, 1>(a, grid, st);
+  else d ? launch_pair<true, 0>(a, grid, st) : launch_pair<false, 0>(a, grid, st);
+  note_launch(1);
+  return cudaGetLastError();
+}
+
 static cudaError_t pack_lane(const PackArgs& a_in, cudaStream_t st, bool u64, bool may_alloc, DevCfg& c) {
   PackArgs a = a_in;
   a.n_tiles = u64 ? (a.n_blocks + 15) / 16 : (a.n_blocks + 31) / 32;
   int shape = 2;
   a.stats = nullptr;
-  if (!u64) {
-    shape = 0;
-    const uint64_t* sv = may_alloc ? lane_stats_dev(c) : nullptr;
-    if (sv) {
-      const volatile uint64_t* hv = c.stats.load(std::memory_order_acquire);
-      const uint64_t bytes = hv[0], blocks = hv[1];
-      shape = (blocks > 0 && bytes <= blocks * (uint64_t)lane::kSmallBlock) ? 1 : 0;
-      a.stats = c.stats_dev;
-    }
-  }
+  if (!u64) shape = pick_window(a, may_alloc, c, (uint64_t)lane::kSmallBlock);
   const int occ = c.lane_ctas[shape];
   const int per_sm = (g_pack_cap > 0 && g_pack_cap < occ) ? g_pack_cap : occ;
   int64_t grid = (int64_t)c.sms * per_sm;
@@ -2187,7 +2411,8 @@ cudaError_t pack(bool u64, const PackArgs& a_in, cudaStream_t st, bool may_alloc
   DevCfg* c = nullptr;
   cudaError_t e = dev_cfg(&c);
   if (e != cudaSuccess) return e;
-  if (g_pack_schedule == 1) return pack_lane(a_in, st, u64, may_alloc, *c);
+  if (g_pack_schedule == 2 && !u64) return pack_pair(a_in, st, may_alloc, *c);
+  if (g_pack_schedule >= 1) return pack_lane(a_in, st, u64, may_alloc, *c);
   if (!u64) {
     PackArgs a = a_in;
     a.n_tiles = (a.n_blocks + kQTile - 1) / kQTile;
@@ -2282,8 +2507,12 @@ int set_knob(int knob, int value) {
       g_pack_cap = value;
       return 0;
     case 2:  // UTL_KNOB_PACK_SCHEDULE
-      if (value != 0 && value != 1) return -1;
+      if (value < 0 || value > 2) return -1;
       g_pack_schedule = value;
+      return 0;
+    case 6:  // UTL_KNOB_PACK_WINDOW
+      if (value < 0 || value > 2) return -1;
+      g_pack_window.store(value, std::memory_order_relaxed);
       return 0;
     case 4:  // UTL_KNOB_SPIN_LIMIT (0 = default)
       if (value < 0 || value > (1 << 30)) return -1;
@@ -2303,6 +2532,7 @@ int get_knob(int knob) {
     case 2: return g_pack_schedule;
     case 4: return (int)g_spin_limit.load(std::memory_order_relaxed);
     case 5: return g_keep_scratch.load(std::memory_order_relaxed);
+    case 6: return g_pack_window.load(std::memory_order_relaxed);
   }
   return -1;
 }

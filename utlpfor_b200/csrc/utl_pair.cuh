@@ -343,33 +343,12 @@ __device__ __forceinline__ int rank_below(const uint32_t (&m)[4], int p) {
   return r;
 }
 
-// Write the block at o (shared memory): header, StreamVByte length, FOR
-// base (thread 0 of the pair), the payload of the thread's two groups, then
-// the exception index and StreamVByte high bits.  Up to 16 exceptions (a
-// position list): each thread handles the exceptions at its own positions
-// (rank = set bits of the block's bitmap below the position), the pair
-// shares the 2-bit length codes (the control bytes) with one shuffle.  More
-// than 16 (a bitmap): the pair walks the bitmap in position order and
-// splits the stores by rank parity.
-template <bool DELTA, bool EXC>
-__device__ void write_block(const lane::Plan& p, const uint4* s4, uint8_t* o, int h, unsigned pm) {
-  if (h == 0) {
-    lane::put_bytes(o, p.header, 4);
-    int m = 4;
-    if (p.exc) {
-      lane::put_bytes(o + 4, (uint32_t)p.svb_len, 2);
-      m = 6;
-    }
-    if (p.forb) lane::put_bytes(o + m, p.base, p.forb);
-  }
+// The exception index and StreamVByte high bits of a block whose payload
+// starts at pay; own holds the exception flags of the thread's positions.
+template <bool DELTA>
+__device__ __forceinline__ void write_exceptions(const lane::Plan& p, const uint4* s4, uint8_t* pay,
+                                                 const uint32_t (&own)[4], int h, unsigned pm) {
   const int bw = p.bw;
-  uint8_t* pay = o + p.p_off;
-  const int d4 = (int)((uintptr_t)pay & 3);
-  uint32_t* pw = (uint32_t*)(pay - d4);
-  const int sh = 32 - 8 * d4;
-  uint32_t own[4] = {0, 0, 0, 0};
-  write_groups<DELTA, EXC>(bw, s4, h, p.base, p.zz, pw, d4, sh, own);
-  if (!EXC || p.exc == 0) return;
   uint32_t bm[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) bm[q] = por(own[q], pm);
@@ -433,6 +412,37 @@ __device__ void write_block(const lane::Plan& p, const uint4* s4, uint8_t* o, in
       }
     }
     if (h == 0 && (rank & 3) && (rank >> 2) < nc) svb[rank >> 2] = (uint8_t)ctrl;
+  }
+}
+
+// Write the block at o (shared memory): header, StreamVByte length, FOR
+// base (thread 0 of the pair), the payload of the thread's two groups, then
+// the exception index and StreamVByte high bits.  Up to 16 exceptions (a
+// position list): each thread handles the exceptions at its own positions
+// (rank = set bits of the block's bitmap below the position), the pair
+// shares the 2-bit length codes (the control bytes) with one shuffle.  More
+// than 16 (a bitmap): the pair walks the bitmap in position order and
+// splits the stores by rank parity.
+template <bool DELTA, bool EXC>
+__device__ void write_block(const lane::Plan& p, const uint4* s4, uint8_t* o, int h, unsigned pm) {
+  if (h == 0) {
+    lane::put_bytes(o, p.header, 4);
+    int m = 4;
+    if (p.exc) {
+      lane::put_bytes(o + 4, (uint32_t)p.svb_len, 2);
+      m = 6;
+    }
+    if (p.forb) lane::put_bytes(o + m, p.base, p.forb);
+  }
+  const int bw = p.bw;
+  uint8_t* pay = o + p.p_off;
+  const int d4 = (int)((uintptr_t)pay & 3);
+  uint32_t* pw = (uint32_t*)(pay - d4);
+  const int sh = 32 - 8 * d4;
+  uint32_t own[4] = {0, 0, 0, 0};
+  write_groups<DELTA, EXC>(bw, s4, h, p.base, p.zz, pw, d4, sh, own);
+  if constexpr (EXC) {
+    if (p.exc) write_exceptions<DELTA>(p, s4, pay, own, h, pm);
   }
 }
 
