@@ -297,6 +297,9 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *     that may allocate (a hint read without waiting), 1 = the large window,
  *     2 = the small window (for batches of at most about 144 bytes a block).
  *     Outputs are the same for every value.
+ *   UTL_KNOB_UNPACK_CTAS_PER_SM: cap on resident CTAs (4 warps each) per SM
+ *     of the persistent unpack kernels, schedules 1-6 (0 = the occupancy
+ *     maximum).
  *   UTL_KNOB_HOST_PIPELINE: the host-buffer batch calls, 0 = one pass
  *     (all copies in, kernels, all copies out); 1 = batches of 64 MiB of
  *     values or more are cut at block boundaries into pieces of
@@ -318,6 +321,7 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
 #define UTL_KNOB_SPIN_LIMIT 4
 #define UTL_KNOB_KEEP_SCRATCH 5
 #define UTL_KNOB_PACK_WINDOW 6
+#define UTL_KNOB_UNPACK_CTAS_PER_SM 7
 UTL_API int utl_set_knob(int knob, int value);
 UTL_API int utl_get_knob(int knob);
 

@@ -36,6 +36,14 @@ def test_graph_replay_matches_eager():
 
 
 def test_tuner_candidates_agree():
-    from utlpfor_b200.tune import tune
-    cfg = tune(log2n=18, write=False)  # asserts that every pack candidate gives the same bytes
-    assert set(cfg["knobs"]) == {"0", "1", "2"}
+    """Every candidate of every knob the tuner sweeps (pack tile size and
+    window, pack and unpack warps per SM, unpack schedule) gives the same
+    bytes and values; the tuner reports a choice for each knob and leaves
+    the knobs as it found them."""
+    from utlpfor_b200._lib import load
+    from utlpfor_b200.tune import KNOBS, tune
+    L = load()
+    before = {k: L.utl_get_knob(int(k)) for k in KNOBS}
+    cfg = tune(log2n=18, write=False)
+    assert set(cfg["knobs"]) == set(KNOBS)
+    assert {k: L.utl_get_knob(int(k)) for k in KNOBS} == before

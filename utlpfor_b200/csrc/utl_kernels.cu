@@ -2258,11 +2258,19 @@ cudaError_t stream_offsets(const uint64_t* block_off, const uint64_t* bstart, in
   return cudaGetLastError();
 }
 
+// UTL_KNOB_UNPACK_CTAS_PER_SM: cap on resident unpack CTAs (of 4 warps) per
+// SM of the persistent unpack kernels (0 = the occupancy maximum).
+static std::atomic<int> g_unpack_cap{0};
+static int unpack_ctas(int occ) {
+  const int cap = g_unpack_cap.load(std::memory_order_relaxed);
+  return (cap > 0 && cap < occ) ? cap : occ;
+}
+
 template <int STAGE, bool AUTO>
 static cudaError_t unpack_pipe(const UnpackArgs& a, cudaStream_t st, int ctas) {
   const size_t psmem = sizeof(QuadPipeSmem<STAGE>);
   const int64_t groups = (a.n_blocks + 7) / 8;
-  int64_t grid = (int64_t)num_sms() * ctas;
+  int64_t grid = (int64_t)num_sms() * unpack_ctas(ctas);
   const int64_t need = (groups + kQWarps - 1) / kQWarps;
   if (grid > need) grid = need;
   unpack_quad_pipe_kernel<STAGE, AUTO><<<(unsigned)grid, kQThreads, psmem, st>>>(a);
@@ -2273,7 +2281,7 @@ template <int STAGE, int NSTAGE, bool AUTO>
 static cudaError_t unpack_tma(const UnpackArgs& a, cudaStream_t st, int ctas) {
   const size_t smem = sizeof(QuadTmaSmem<STAGE, NSTAGE>);
   const int64_t groups = (a.n_blocks + 7) / 8;
-  int64_t grid = (int64_t)num_sms() * ctas;
+  int64_t grid = (int64_t)num_sms() * unpack_ctas(ctas);
   const int64_t need = (groups + kQWarps - 1) / kQWarps;
   if (grid > need) grid = need;
   unpack_quad_tma_kernel<STAGE, NSTAGE, AUTO><<<(unsigned)grid, kQThreads, smem, st>>>(a);
@@ -2510,6 +2518,10 @@ int set_knob(int knob, int value) {
       if (value < 0 || value > 2) return -1;
       g_pack_schedule = value;
       return 0;
+    case 7:  // UTL_KNOB_UNPACK_CTAS_PER_SM (0 = occupancy maximum)
+      if (value < 0 || value > 32) return -1;
+      g_unpack_cap.store(value, std::memory_order_relaxed);
+      return 0;
     case 6:  // UTL_KNOB_PACK_WINDOW
       if (value < 0 || value > 2) return -1;
       g_pack_window.store(value, std::memory_order_relaxed);
@@ -2533,6 +2545,7 @@ int get_knob(int knob) {
     case 4: return (int)g_spin_limit.load(std::memory_order_relaxed);
     case 5: return g_keep_scratch.load(std::memory_order_relaxed);
     case 6: return g_pack_window.load(std::memory_order_relaxed);
+    case 7: return g_unpack_cap.load(std::memory_order_relaxed);
   }
   return -1;
 }
