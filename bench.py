@@ -788,7 +788,29 @@ def main():
                 lat_p.append(t1 - t0)
                 lat_u.append(t2 - t1)
         tot = sum(lat_p) + sum(lat_u)
+        # the same calls from 8 host threads through a pool of 8 contexts
+        pool = U.CompressorPool(8)
+        n_thr = 8
+        per = max(1, (hv_n // 128) // n_thr)
+
+        def pool_worker(k):
+            for i in range(k * per, (k + 1) * per):
+                blk = hv[128 * i:128 * i + 128]
+                pk = pool.PackUint32(flag, blk)
+                got, _ = pool.UnpackUint32(pk)
+                assert np.array_equal(got, blk)
+
+        pool_worker(0)  # warm every context
+        ths = [threading.Thread(target=pool_worker, args=(k,)) for k in range(n_thr)]
+        tp0 = time.perf_counter()
+        for t_ in ths:
+            t_.start()
+        for t_ in ths:
+            t_.join()
+        pool_s = time.perf_counter() - tp0
+        pool.close()
         plain = {"GBps": 2 * 4 * hv_n / tot / 1e9, "unit": "GB/s (round-trip uncompressed)", "blocks": hv_n // 128,
+                 "pooled_8_threads_GBps": 2 * 4 * 128 * per * n_thr / pool_s / 1e9,
                  "pack_us_p50": 1e6 * float(np.median(lat_p)), "pack_us_p99": 1e6 * float(np.percentile(lat_p, 99)),
                  "unpack_us_p50": 1e6 * float(np.median(lat_u)),
                  "unpack_us_p99": 1e6 * float(np.percentile(lat_u, 99)),

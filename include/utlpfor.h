@@ -131,6 +131,32 @@ UTL_API int utl_codec_unpack_u64(utl_codec *c, const uint8_t *src, size_t src_le
 UTL_API int utl_codec_get_u64(utl_codec *c, int pos, const uint8_t *src,
                       size_t src_len, uint64_t *value, int *overflow_pos);
 
+/* A pool of per-call contexts for servers that call from many host threads
+ * at once (the reference's Compressor32/64 are not safe for concurrent use,
+ * compressor.go:8,63, so a Go server keeps one per goroutine or a
+ * sync.Pool of them; this is that pool on the C side).  Each of the
+ * n_contexts contexts owns a CUDA stream and mapped pinned staging; a call
+ * takes a free one, runs the per-call kernel on its stream and returns it,
+ * so calls from different threads overlap on the GPU.  All calls are
+ * thread-safe and behave exactly as utl_pack_u32 etc.  The pool belongs to
+ * the device current at utl_pool_new; calls switch to it for their
+ * duration.  No counterpart function in the reference. */
+typedef struct utl_pool utl_pool;
+UTL_API int utl_pool_new(int n_contexts, utl_pool **out);
+UTL_API void utl_pool_free(utl_pool *p);
+UTL_API int utl_pool_pack_u32(utl_pool *p, uint8_t flag, const uint32_t *values, int n, uint8_t *dst,
+                              size_t dst_cap, size_t *out_len);
+UTL_API int utl_pool_unpack_u32(utl_pool *p, const uint8_t *src, size_t src_len, uint32_t *values, int *count,
+                                size_t *consumed, int *overflow_pos);
+UTL_API int utl_pool_get_u32(utl_pool *p, int pos, const uint8_t *src, size_t src_len, uint32_t *value,
+                             int *overflow_pos);
+UTL_API int utl_pool_pack_u64(utl_pool *p, uint8_t flag, const uint64_t *values, int n, uint8_t *dst,
+                              size_t dst_cap, size_t *out_len);
+UTL_API int utl_pool_unpack_u64(utl_pool *p, const uint8_t *src, size_t src_len, uint64_t *values, int *count,
+                                size_t *consumed, int *overflow_pos);
+UTL_API int utl_pool_get_u64(utl_pool *p, int pos, const uint8_t *src, size_t src_len, uint64_t *value,
+                             int *overflow_pos);
+
 /* ==================== batched (device buffers) ==================== */
 /* One launch packs, unpacks or queries the blocks of many streams of
  * uneven length.  The reference has no batched form; these replace the

@@ -29,8 +29,8 @@ def _p(t):
     return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
 
 
-@pytest.mark.parametrize("is64,schedule", [(False, 1), (False, 0), (True, 1), (True, 0)],
-                         ids=["u32_lane", "u32_quad", "u64_lane", "u64_warp"])
+@pytest.mark.parametrize("is64,schedule", [(False, 2), (False, 1), (False, 0), (True, 1), (True, 0)],
+                         ids=["u32_pair", "u32_lane", "u32_quad", "u64_lane", "u64_warp"])
 def test_pack_wait_expires_and_reports_timeout(is64, schedule):
     import time
 

@@ -20,7 +20,7 @@ __all__ = [
     "PackUint32", "UnpackUint32", "GetUint32", "PackUint64", "UnpackUint64", "GetUint64",
     "BlockLength", "Header", "MaxBlockLength32", "MaxBlockLength64",
     "ScratchLen", "ScratchLenNoInPlace", "ScratchLen64",
-    "Compressor32", "Compressor64", "NewUint32", "NewUint64",
+    "Compressor32", "Compressor64", "NewUint32", "NewUint64", "CompressorPool",
 ]
 
 # Flags, utlpfor.go:24-68
@@ -99,7 +99,7 @@ def _u8(src):
     return b, b.ctypes.data_as(C.POINTER(C.c_uint8))
 
 
-def _pack(is64, flag, values, dst, codec=None):
+def _pack(is64, flag, values, dst, codec=None, kind="codec"):
     L = load()
     dt, P = (np.uint64, C.c_uint64) if is64 else (np.uint32, C.c_uint32)
     v = np.ascontiguousarray(values, dtype=dt)
@@ -109,7 +109,7 @@ def _pack(is64, flag, values, dst, codec=None):
     args = (flag & 0xFF, v.ctypes.data_as(C.POINTER(P)), len(v), out.ctypes.data_as(C.POINTER(C.c_uint8)),
             cap, C.byref(n))
     if codec is not None:
-        rc = (L.utl_codec_pack_u64 if is64 else L.utl_codec_pack_u32)(codec, *args)
+        rc = getattr(L, "utl_%s_pack_%s" % (kind, "u64" if is64 else "u32"))(codec, *args)
     else:
         rc = (L.utl_pack_u64 if is64 else L.utl_pack_u32)(*args)
     _raise(rc)
@@ -122,7 +122,7 @@ def _pack(is64, flag, values, dst, codec=None):
     return bytearray(block)
 
 
-def _unpack(is64, src, codec=None):
+def _unpack(is64, src, codec=None, kind="codec"):
     L = load()
     b, p = _u8(src)
     dt, P = (np.uint64, C.c_uint64) if is64 else (np.uint32, C.c_uint32)
@@ -130,21 +130,21 @@ def _unpack(is64, src, codec=None):
     cnt, cons, ovf = C.c_int(0), C.c_size_t(0), C.c_int(0)
     args = (p, len(b), out.ctypes.data_as(C.POINTER(P)), C.byref(cnt), C.byref(cons), C.byref(ovf))
     if codec is not None:
-        rc = (L.utl_codec_unpack_u64 if is64 else L.utl_codec_unpack_u32)(codec, *args)
+        rc = getattr(L, "utl_%s_unpack_%s" % (kind, "u64" if is64 else "u32"))(codec, *args)
     else:
         rc = (L.utl_unpack_u64 if is64 else L.utl_unpack_u32)(*args)
     _raise(rc, ovf.value)
     return out[:cnt.value].copy(), cons.value
 
 
-def _get(is64, pos, src, codec=None):
+def _get(is64, pos, src, codec=None, kind="codec"):
     L = load()
     b, p = _u8(src)
     val = C.c_uint64(0) if is64 else C.c_uint32(0)
     ovf = C.c_int(0)
     args = (int(pos), p, len(b), C.byref(val), C.byref(ovf))
     if codec is not None:
-        rc = (L.utl_codec_get_u64 if is64 else L.utl_codec_get_u32)(codec, *args)
+        rc = getattr(L, "utl_%s_get_%s" % (kind, "u64" if is64 else "u32"))(codec, *args)
     else:
         rc = (L.utl_get_u64 if is64 else L.utl_get_u32)(*args)
     _raise(rc, ovf.value)
@@ -238,6 +238,51 @@ class Compressor32(_Codec):
 class Compressor64(_Codec):
     """Compressor64 (compressor.go:63)."""
     _is64 = True
+
+
+class CompressorPool:
+    """A pool of per-call GPU contexts shared by any number of threads.
+
+    The reference's Compressor32/64 must not be used concurrently
+    (compressor.go:8,63); a server calling from many threads would keep one
+    per thread or a pool of them.  This is that pool: n contexts, each with
+    its own CUDA stream and mapped pinned staging; every call takes a free
+    one, so calls from different threads overlap on the GPU.  Methods are
+    thread-safe and return exactly what PackUint32/UnpackUint32/GetUint32
+    (and the 64-bit forms) return."""
+
+    def __init__(self, n_contexts=8):
+        h = C.c_void_p()
+        _raise(load().utl_pool_new(int(n_contexts), C.byref(h)))
+        self._h = h
+        self.n_contexts = int(n_contexts)
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            load().utl_pool_free(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def PackUint32(self, flag, values, dst=None):
+        return _pack(False, flag, values, dst, self._h, "pool")
+
+    def UnpackUint32(self, src):
+        return _unpack(False, src, self._h, "pool")
+
+    def GetUint32(self, pos, src):
+        return _get(False, pos, src, self._h, "pool")
+
+    def PackUint64(self, flag, values, dst=None):
+        return _pack(True, flag, values, dst, self._h, "pool")
+
+    def UnpackUint64(self, src):
+        return _unpack(True, src, self._h, "pool")
+
+    def GetUint64(self, pos, src):
+        return _get(True, pos, src, self._h, "pool")
 
 
 def NewUint32():

@@ -37,6 +37,14 @@ SIGNATURES = [
     ("utl_codec_pack_u64", C.c_int, [VP, C.c_uint8, PU64, C.c_int, P8, C.c_size_t, SZ]),
     ("utl_codec_unpack_u64", C.c_int, [VP, P8, C.c_size_t, PU64, PI, SZ, PI]),
     ("utl_codec_get_u64", C.c_int, [VP, C.c_int, P8, C.c_size_t, PU64, PI]),
+    ("utl_pool_new", C.c_int, [C.c_int, C.POINTER(VP)]),
+    ("utl_pool_free", None, [VP]),
+    ("utl_pool_pack_u32", C.c_int, [VP, C.c_uint8, PU32, C.c_int, P8, C.c_size_t, SZ]),
+    ("utl_pool_unpack_u32", C.c_int, [VP, P8, C.c_size_t, PU32, PI, SZ, PI]),
+    ("utl_pool_get_u32", C.c_int, [VP, C.c_int, P8, C.c_size_t, PU32, PI]),
+    ("utl_pool_pack_u64", C.c_int, [VP, C.c_uint8, PU64, C.c_int, P8, C.c_size_t, SZ]),
+    ("utl_pool_unpack_u64", C.c_int, [VP, P8, C.c_size_t, PU64, PI, SZ, PI]),
+    ("utl_pool_get_u64", C.c_int, [VP, C.c_int, P8, C.c_size_t, PU64, PI]),
     ("utl_count_blocks", C.c_int64, [PU64, C.c_int]),
     ("utl_batch_plan", C.c_int, [VP, C.c_int, VP, VP]),
     ("utl_pack_scratch_bytes", C.c_size_t, [C.c_int64]),

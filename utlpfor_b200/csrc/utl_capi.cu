@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <atomic>
 #include <mutex>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -427,6 +428,123 @@ int utl_codec_unpack_u64(utl_codec* c, const uint8_t* src, size_t src_len, uint6
 int utl_codec_get_u64(utl_codec* c, int pos, const uint8_t* src, size_t src_len, uint64_t* value, int* overflow_pos) {
   if (!c) return UTL_ERR_ARG;
   return get_call(&c->ctx, true, pos, src, src_len, value, overflow_pos);
+}
+
+// ---------------------------------------------------------------------------
+// pool of per-call contexts for many host threads
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+// A fixed set of contexts (each: CUDA stream, mapped pinned staging, device
+// scratch) shared by any number of host threads.  A call takes a free
+// context (try-lock, starting at a rotating index so callers spread over
+// the set), runs the per-call kernel on its stream and gives it back; calls
+// on different contexts overlap on the GPU.
+struct utl_pool {
+  int device = 0;
+  int n = 0;
+  Ctx* ctx = nullptr;
+  std::atomic<int>* busy = nullptr;
+  std::atomic<uint32_t> next{0};
+};
+
+namespace {
+struct PoolLease {
+  utl_pool* p;
+  int i = -1;
+  int prev_dev = -1;
+  explicit PoolLease(utl_pool* pool) : p(pool) {
+    const uint32_t start = p->next.fetch_add(1, std::memory_order_relaxed);
+    for (uint64_t t = 0;; t++) {
+      const int k = (int)((start + t) % (uint32_t)p->n);
+      int z = 0;
+      if (p->busy[k].load(std::memory_order_relaxed) == 0 &&
+          p->busy[k].compare_exchange_strong(z, 1, std::memory_order_acquire)) {
+        i = k;
+        break;
+      }
+      if ((t + 1) % (uint64_t)p->n == 0) std::this_thread::yield();
+    }
+    int cur = 0;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != p->device) {
+      prev_dev = cur;
+      cudaSetDevice(p->device);
+    }
+  }
+  ~PoolLease() {
+    if (prev_dev >= 0) cudaSetDevice(prev_dev);
+    p->busy[i].store(0, std::memory_order_release);
+  }
+  Ctx* ctx() { return &p->ctx[i]; }
+};
+}  // namespace
+
+extern "C" {
+
+int utl_pool_new(int n_contexts, utl_pool** out) {
+  if (!out || n_contexts <= 0 || n_contexts > 1024) return UTL_ERR_ARG;
+  *out = nullptr;
+  utl_pool* p = new utl_pool();
+  p->n = n_contexts;
+  p->ctx = new Ctx[n_contexts];
+  p->busy = new std::atomic<int>[n_contexts];
+  int rc = UTL_OK;
+  cudaError_t e = cudaGetDevice(&p->device);
+  if (e != cudaSuccess) rc = cuda_fail(e);
+  for (int k = 0; k < n_contexts; k++) {
+    p->busy[k].store(0);
+    if (rc == UTL_OK) rc = p->ctx[k].init();
+  }
+  if (rc != UTL_OK) {
+    utl_pool_free(p);
+    return rc;
+  }
+  *out = p;
+  return UTL_OK;
+}
+void utl_pool_free(utl_pool* p) {
+  if (!p) return;
+  for (int k = 0; k < p->n; k++) p->ctx[k].destroy();
+  delete[] p->ctx;
+  delete[] p->busy;
+  delete p;
+}
+int utl_pool_pack_u32(utl_pool* p, uint8_t flag, const uint32_t* values, int n, uint8_t* dst, size_t dst_cap,
+                      size_t* out_len) {
+  if (!p) return UTL_ERR_ARG;
+  PoolLease l(p);
+  return pack_call(l.ctx(), false, flag, values, n, dst, dst_cap, out_len);
+}
+int utl_pool_unpack_u32(utl_pool* p, const uint8_t* src, size_t src_len, uint32_t* values, int* count,
+                        size_t* consumed, int* overflow_pos) {
+  if (!p) return UTL_ERR_ARG;
+  PoolLease l(p);
+  return unpack_call(l.ctx(), false, src, src_len, values, count, consumed, overflow_pos);
+}
+int utl_pool_get_u32(utl_pool* p, int pos, const uint8_t* src, size_t src_len, uint32_t* value, int* overflow_pos) {
+  if (!p || !value) return UTL_ERR_ARG;
+  uint64_t v = 0;
+  PoolLease l(p);
+  const int rc = get_call(l.ctx(), false, pos, src, src_len, &v, overflow_pos);
+  if (rc == UTL_OK) *value = (uint32_t)v;
+  return rc;
+}
+int utl_pool_pack_u64(utl_pool* p, uint8_t flag, const uint64_t* values, int n, uint8_t* dst, size_t dst_cap,
+                      size_t* out_len) {
+  if (!p) return UTL_ERR_ARG;
+  PoolLease l(p);
+  return pack_call(l.ctx(), true, flag, values, n, dst, dst_cap, out_len);
+}
+int utl_pool_unpack_u64(utl_pool* p, const uint8_t* src, size_t src_len, uint64_t* values, int* count,
+                        size_t* consumed, int* overflow_pos) {
+  if (!p) return UTL_ERR_ARG;
+  PoolLease l(p);
+  return unpack_call(l.ctx(), true, src, src_len, values, count, consumed, overflow_pos);
+}
+int utl_pool_get_u64(utl_pool* p, int pos, const uint8_t* src, size_t src_len, uint64_t* value, int* overflow_pos) {
+  if (!p) return UTL_ERR_ARG;
+  PoolLease l(p);
+  return get_call(l.ctx(), true, pos, src, src_len, value, overflow_pos);
 }
 
 // ---------------------------------------------------------------------------

@@ -1711,11 +1711,9 @@ __device__ __forceinline__ int pair_load_tile(const PackArgs& a, int64_t tile, u
   if (whole && mis == 0) {
     const uint8_t* src = (const uint8_t*)(vals + f0) + 16 * lane;
     uint8_t* dst = inb + 16 * lane;
+    // block k's 32 chunks, chunk l from lane l
 #pragma unroll 8
-    for (int k = 0; k < 16; k++) {
-      cp_async16(dst + k * pair::kSlot, src + 512 * k);
-      cp_async16(dst + k * pair::kSlot + 256, src + 512 * k + 256);
-    }
+    for (int k = 0; k < 16; k++) cp_async16(dst + k * pair::kSlot, src + 512 * k);
   } else if (whole && (((uintptr_t)vals) & 15) == 0 && f0 - (uint64_t)mis >= a.val_off[0] &&
              f0 - (uint64_t)mis + 16 * kBlock + 4 <= a.val_off[a.n_streams]) {
     pair_issue_shifted(inb, (const uint8_t*)(vals + f0 - mis), lane);
