@@ -306,12 +306,13 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *     32 blocks; 2 = persistent warps with the next group's bytes in
  *     flight (cp.async double buffer), staging up to 528 bytes a block;
  *     3 = the same staging up to 264 bytes a block (more warps resident);
- *     1 = 3 or 2 by the batch's mean block length, decided on the device;
+ *     1 = 3 or 2 by the batch's mean block length, decided on the device
+ *     (the default);
  *     5 = persistent warps staging each group of 8 blocks with one TMA bulk
  *     copy, three groups in flight, up to 264 bytes a block, with the
  *     register fast path for blocks of at most 16 exceptions; 6 = the same
  *     with two groups of up to 528 bytes a block in flight; 4 = 5 or 6 by
- *     the batch's mean block length, decided on the device (the default).
+ *     the batch's mean block length, decided on the device.
  *   UTL_KNOB_PACK_CTAS_PER_SM: cap on resident pack CTAs per SM (0 = the
  *     occupancy maximum).
  *   UTL_KNOB_PACK_SCHEDULE: uint32 pack kernel, 0 = four threads per block
@@ -326,6 +327,10 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *   UTL_KNOB_UNPACK_CTAS_PER_SM: cap on resident CTAs (4 warps each) per SM
  *     of the persistent unpack kernels, schedules 1-6 (0 = the occupancy
  *     maximum).
+ *   UTL_KNOB_UNPACK64_SCHEDULE: the uint64 unpack kernel, 0 = a warp per
+ *     block; 1 = an octet of lanes per block (one quad per uint32
+ *     sub-block, both decoded at once), 4 blocks per warp staged by TMA bulk
+ *     copies, two groups in flight (the default); 2 = the same with three.
  *   UTL_KNOB_HOST_PIPELINE: the host-buffer batch calls, 0 = one pass
  *     (all copies in, kernels, all copies out); 1 = batches of 64 MiB of
  *     values or more are cut at block boundaries into pieces of
@@ -348,6 +353,7 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
 #define UTL_KNOB_KEEP_SCRATCH 5
 #define UTL_KNOB_PACK_WINDOW 6
 #define UTL_KNOB_UNPACK_CTAS_PER_SM 7
+#define UTL_KNOB_UNPACK64_SCHEDULE 8
 UTL_API int utl_set_knob(int knob, int value);
 UTL_API int utl_get_knob(int knob);
 

@@ -996,6 +996,235 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_tma_kernel(UnpackArg
   }
 }
 
+// ------------------------------------------------------------------------
+// uint64 unpack with TMA staging: an octet of lanes per uint64 block, 4
+// blocks per warp.  The octet's first quad decodes the block's first
+// uint32 sub-block (the only one of a FOR64 or fit-32 block), its second
+// quad the upper-halves sub-block of a two-block pair at the same time
+// (unpackUint64Block, uint64.go:191-266); the halves meet by one shuffle
+// per pair of values and every lane stores 16-byte pairs of uint64.
+// ------------------------------------------------------------------------
+constexpr int kO64Stage = 4224;  // a group of 4 blocks of up to ~1 KB (two-block pairs of width 32)
+
+__device__ __forceinline__ TmaGroup tma_group_load4(const UnpackArgs& a, int64_t g, int lane) {
+  TmaGroup t;
+  const int64_t b0 = g * 4;
+  const int nb = b0 < a.n_blocks ? (int)min((int64_t)4, a.n_blocks - b0) : 0;
+  t.off = (nb > 0 && lane <= nb) ? a.block_off[b0 + lane] : 0ull;
+  t.s0 = (nb > 0 && lane == 0) ? stream_of(a.block_start, a.n_streams, b0) : 0;
+  return t;
+}
+__device__ __forceinline__ int tma_group_nb4(const UnpackArgs& a, int64_t g) {
+  const int64_t b0 = g * 4;
+  return b0 < a.n_blocks ? (int)min((int64_t)4, a.n_blocks - b0) : 0;
+}
+template <int STAGE>
+__device__ __forceinline__ bool tma_group_fits64(const UnpackArgs& a, const TmaGroup& t, int nb, int lane) {
+  if (nb <= 0) return false;
+  const uint64_t next = __shfl_down_sync(kFull, t.off, 1);
+  const bool ok = lane >= nb || (next >= t.off && next - t.off <= (uint64_t)kMaxBlock64 && next <= a.packed_len);
+  const uint64_t o0 = __shfl_sync(kFull, t.off, 0), o1 = __shfl_sync(kFull, t.off, nb);
+  const int ph = (int)(((uintptr_t)a.packed + o0) & 15);
+  return __all_sync(kFull, ok) && (int64_t)(o1 - o0) + ph + 16 <= STAGE;
+}
+
+// Decode and store uint64 block at staging offset blk (len bytes) by an
+// octet (quad qh of it: 0 first sub-block, 1 upper halves).  Returns the
+// status (octet-uniform) and overflow position.
+__device__ __forceinline__ void oct64_block(const SmemBytes& sb, int blk, int len, uint64_t* op, int want,
+                                            uint32_t* patch, int qh, int j, int lane, int& status, int& ovf) {
+  const unsigned qm = quad::quad_mask(lane);
+  const unsigned om = 0xFFu << (lane & 24);
+  status = kOK;
+  ovf = 0;
+  if (len < 4) { status = kErrInvalidBuffer; return; }
+  const uint32_t h = sb.u32(blk);
+  if (((h >> 13) & 3) != 3) { status = kErrUnsupportedType; return; }
+  const int forw = (int)((h >> 15) & 3);
+  const int exc = (int)(h >> 24);
+  uint32_t x[8][4];
+  if (!(h & kHdrCombine)) {
+    // FOR64 or fit-32: one sub-block, decoded by the first quad
+    uint64_t base = 0;
+    if (forw == 3) {
+      const int off = 4 + (exc > 0 ? 2 : 0);
+      if (len < off + 8) { status = kErrInvalidBuffer; return; }
+      base = sb.u64(blk + off);
+    }
+    quad::QResult r{kOK, 0, 0, 0};
+    if (qh == 0) r = quad::quad_unpack_block(sb, blk, len, true, x, patch, j, qm);
+    int st = r.status, ov = r.ovf;
+    if (st == kOK && (r.count != want || r.consumed != len)) st = kErrCountMismatch;
+    st = __shfl_sync(om, st, lane & 24);
+    ov = __shfl_sync(om, ov, lane & 24);
+    status = st;
+    ovf = ov;
+    if (st != kOK || qh != 0) return;
+    if (want == kBlock) {
+#pragma unroll
+      for (int v = 0; v < 8; v++) {
+        const int i = 16 * v + 4 * j;
+        __stcs((ulonglong2*)(op + i), make_ulonglong2(base + x[v][0], base + x[v][1]));
+        __stcs((ulonglong2*)(op + i + 2), make_ulonglong2(base + x[v][2], base + x[v][3]));
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < 8; v++)
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          if (16 * v + 4 * j + k < want) op[16 * v + 4 * j + k] = base + x[v][k];
+    }
+    return;
+  }
+  // two-block pair: the first sub-block's length from its header (what its
+  // decode consumes when it is valid), then both sub-blocks at once
+  const int p1 = 4 + (exc > 0 ? 2 : 0) + ((1 << forw) >> 1) + 2;  // meta: its block2Len field ends here
+  const int bw1 = (int)((h >> 8) & 31) * 4;
+  const int c1 = (h & 0xFF) == 0 ? 4 : p1 + 16 * bw1 + (exc > 0 ? min(exc, 16) + (int)sb.u16(blk + 4) : 0);
+  const int b2len = len >= p1 ? (int)sb.u16(blk + p1 - 2) : 0;
+  const bool hi_ok = len >= p1 && c1 + b2len <= len;  // (an empty first sub-block consumes its header only)
+  quad::QResult r{kOK, 0, 0, 0};
+  if (qh == 0) r = quad::quad_unpack_block(sb, blk, len, true, x, patch, j, qm);
+  else if (hi_ok) r = quad::quad_unpack_block(sb, blk + c1, b2len, true, x, patch, j, qm);
+  const int st1 = __shfl_sync(om, r.status, lane & 24), ov1 = __shfl_sync(om, r.ovf, lane & 24);
+  const int n1 = __shfl_sync(om, r.count, lane & 24), cons1 = __shfl_sync(om, r.consumed, lane & 24);
+  const int st2 = __shfl_sync(om, r.status, (lane & 24) + 4), ov2 = __shfl_sync(om, r.ovf, (lane & 24) + 4);
+  const int n2 = __shfl_sync(om, r.count, (lane & 24) + 4);
+  // the reference's order: first sub-block, bounds of the pair, second
+  // sub-block, equal counts (uint64.go:226-262)
+  if (st1 != kOK) { status = st1; ovf = ov1; return; }
+  if (len < p1 || cons1 + b2len > len) { status = kErrInvalidBuffer; return; }
+  if (st2 != kOK) { status = st2; ovf = ov2; return; }
+  if (n2 != n1) { status = kErrInvalidBuffer; return; }
+  if (n1 != want || cons1 + b2len != len) { status = kErrCountMismatch; return; }
+  // lane j of the first quad stores values 4j, 4j+1 of each row, lane j of
+  // the second quad 4j+2, 4j+3: each sends the partner the halves it needs
+  const int i0 = (qh == 0) ? 0 : 2;
+#pragma unroll
+  for (int v = 0; v < 8; v++) {
+    const uint32_t a0 = __shfl_xor_sync(om, qh == 0 ? x[v][2] : x[v][0], 4);
+    const uint32_t a1 = __shfl_xor_sync(om, qh == 0 ? x[v][3] : x[v][1], 4);
+    const uint64_t v0 = qh == 0 ? ((uint64_t)a0 << 32 | x[v][0]) : ((uint64_t)x[v][2] << 32 | a0);
+    const uint64_t v1 = qh == 0 ? ((uint64_t)a1 << 32 | x[v][1]) : ((uint64_t)x[v][3] << 32 | a1);
+    const int i = 16 * v + 4 * j + i0;
+    if (want == kBlock) {
+      __stcs((ulonglong2*)(op + i), make_ulonglong2(v0, v1));
+    } else {
+      if (i < want) op[i] = v0;
+      if (i + 1 < want) op[i + 1] = v1;
+    }
+  }
+}
+
+template <int NSTAGE>
+struct Oct64Smem {
+  uint4 stage[kQWarps][NSTAGE][(kO64Stage + kQStagePad) / 16];
+  uint4 patch[kQWarps][8][kBlock / 4 + 1];
+  uint64_t bar[kQWarps][NSTAGE];
+};
+
+template <int NSTAGE>
+__global__ void __launch_bounds__(kQThreads, 4) unpack_oct64_tma_kernel(UnpackArgs a) {
+  extern __shared__ uint4 smem4[];
+  Oct64Smem<NSTAGE>& S = *(Oct64Smem<NSTAGE>*)smem4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ob = lane >> 3, qh = (lane >> 2) & 1, j = lane & 3;  // octet = block of the group
+  const int64_t n_groups = (a.n_blocks + 3) / 4;
+  const int64_t stride = (int64_t)gridDim.x * kQWarps;
+  int64_t g = (int64_t)blockIdx.x * kQWarps + warp;
+  if (g >= n_groups) return;
+  uint32_t* patch = (uint32_t*)S.patch[warp][lane >> 2];
+  if (lane == 0) {
+#pragma unroll
+    for (int s = 0; s < NSTAGE; s++) tma::mbar_init(&S.bar[warp][s], 1);
+    tma::mbar_init_fence();
+  }
+  __syncwarp();
+  const uint32_t lim = a.spin_limit;
+  uint32_t pend = 0, phase = 0, fits = 0;
+  TmaGroup gq[NSTAGE];
+#pragma unroll
+  for (int k = 0; k < NSTAGE; k++) {
+    gq[k] = tma_group_load4(a, g + k * stride, lane);
+    if (tma_group_fits64<kO64Stage>(a, gq[k], tma_group_nb4(a, g + k * stride), lane)) fits |= 1u << k;
+  }
+#pragma unroll
+  for (int k = 0; k < NSTAGE - 1; k++)
+    if (((fits >> k) & 1u) && stage_issue(a, gq[k], tma_group_nb4(a, g + k * stride), S.stage[warp][k],
+                                          &S.bar[warp][k], lane))
+      pend |= 1u << k;
+  bool timed_out = false;
+  int st = 0;
+  for (; g < n_groups; g += stride) {
+    const int sn = st == 0 ? NSTAGE - 1 : st - 1;
+    if (((fits >> (NSTAGE - 1)) & 1u) &&
+        stage_issue(a, gq[NSTAGE - 1], tma_group_nb4(a, g + (NSTAGE - 1) * stride), S.stage[warp][sn],
+                    &S.bar[warp][sn], lane))
+      pend |= 1u << sn;
+    if ((pend >> st) & 1u) {
+      if (!tma::mbar_wait(&S.bar[warp][st], (phase >> st) & 1u, lim)) {
+        timed_out = true;
+        break;
+      }
+      pend &= ~(1u << st);
+      phase ^= 1u << st;
+    }
+    __syncwarp();
+    const int nb = tma_group_nb4(a, g);
+    const bool cur_fits = fits & 1u;
+    const uint64_t off0 = __shfl_sync(kFull, gq[0].off, 0);
+    const uint64_t s = __shfl_sync(kFull, gq[0].off, ob), e = __shfl_sync(kFull, gq[0].off, ob + 1);
+    const bool bad = e < s || e - s > (uint64_t)kMaxBlock64 || e > a.packed_len;
+    const int64_t b = g * 4 + ob;
+    const int s0 = __shfl_sync(kFull, gq[0].s0, 0);
+    const int rounds = cur_fits ? 1 : nb;
+    uint4* stg = S.stage[warp][st];
+#pragma unroll 1
+    for (int rd = 0; rd < rounds; rd++) {
+      if (!cur_fits) {
+        const uint64_t rs = __shfl_sync(kFull, gq[0].off, rd), re = __shfl_sync(kFull, gq[0].off, rd + 1);
+        __syncwarp();
+        if (re >= rs && re - rs <= (uint64_t)kMaxBlock64 && re <= a.packed_len)
+          stage_bytes(stg, a.packed, a.packed_len, rs, re, lane, 32);
+        __syncwarp();
+      }
+      if (cur_fits ? ob < nb : ob == rd) {
+        uint64_t first;
+        int want;
+        span_in(a.val_off, a.block_start, stream_from(a.block_start, a.n_streams, s0, b), b, &first, &want);
+        int status = kOK, ovf = 0;
+        if (bad) {
+          status = kErrCountMismatch;
+        } else {
+          const int len = (int)(e - s);
+          const int blk = cur_fits ? (int)(((uintptr_t)a.packed + off0) & 15) + (int)(s - off0)
+                                   : (int)(((uintptr_t)a.packed + s) & 15);
+          oct64_block(SmemBytes{(const uint32_t*)stg}, blk, len, (uint64_t*)a.values + first, want, patch, qh, j,
+                      lane, status, ovf);
+        }
+        if ((lane & 7) == 0) {
+          if (a.block_status) a.block_status[b] = status | (ovf << 8);
+          if (status != kOK && a.err) atomicOr(a.err, 1u << status);
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < NSTAGE - 1; k++) gq[k] = gq[k + 1];
+    fits >>= 1;
+    gq[NSTAGE - 1] = tma_group_load4(a, g + NSTAGE * stride, lane);
+    if (tma_group_fits64<kO64Stage>(a, gq[NSTAGE - 1], tma_group_nb4(a, g + NSTAGE * stride), lane))
+      fits |= 1u << (NSTAGE - 1);
+    st = st == NSTAGE - 1 ? 0 : st + 1;
+  }
+  if (timed_out) {
+    if (lane == 0 && a.err) atomicOr(a.err, 1u << 10);
+#pragma unroll
+    for (int s2 = 0; s2 < NSTAGE; s2++)
+      if ((pend >> s2) & 1u) tma::mbar_wait(&S.bar[warp][s2], (phase >> s2) & 1u, lim);
+  }
+}
+
 struct QuadPackSmem {
   uint32_t hb[kQTile][kBlock];
   uint32_t xs[kQTile][kBlock];
@@ -2160,6 +2389,7 @@ struct DevCfg {
   int pipe_wide_ctas = 0;        // unpack_quad_pipe_kernel, wide staging
   int tma_ctas = 0;              // unpack_quad_tma_kernel, narrow staging (3 stages)
   int tma_wide_ctas = 0;         // unpack_quad_tma_kernel, wide staging (2 stages)
+  int oct64_ctas[2] = {0, 0};    // unpack_oct64_tma_kernel, 2 / 3 stages
   int pack_ctas[2] = {0, 0};     // pack_kernel<false/true>
   // Mapped pinned pair the uint32 lane pack's last block fills with the
   // batch's packed bytes and block count; the next allocating launch on
@@ -2256,6 +2486,9 @@ cudaError_t stream_offsets(const uint64_t* block_off, const uint64_t* bstart, in
   return cudaGetLastError();
 }
 
+// UTL_KNOB_UNPACK64_SCHEDULE: 0 = warp per block, 1 / 2 = an octet per
+// block with TMA staging, two / three groups in flight per warp.
+static std::atomic<int> g_unpack64_schedule{1};
 // UTL_KNOB_UNPACK_CTAS_PER_SM: cap on resident unpack CTAs (of 4 warps) per
 // SM of the persistent unpack kernels (0 = the occupancy maximum).
 static std::atomic<int> g_unpack_cap{0};
@@ -2287,7 +2520,7 @@ static cudaError_t unpack_tma(const UnpackArgs& a, cudaStream_t st, int ctas) {
   return cudaGetLastError();
 }
 // UTL_KNOB_UNPACK_SCHEDULE (include/utlpfor.h)
-static int g_unpack_schedule = 4;
+static int g_unpack_schedule = 1;
 static int g_pack_cap = 0;
 static int g_pack_schedule = 1;
 // Test knobs: the polls of every bounded wait (0 = the default 2^22), and
@@ -2351,6 +2584,10 @@ static cudaError_t setup_device(int dev, DevCfg& c) {
   if ((e = set_smem(unpack_quad_tma_kernel<kPStageWide, 2, false>, tw)) != cudaSuccess) return e;
   c.tma_ctas = occupancy(unpack_quad_tma_kernel<kPStageNarrow, 3, false>, kQThreads, tn);
   c.tma_wide_ctas = occupancy(unpack_quad_tma_kernel<kPStageWide, 2, false>, kQThreads, tw);
+  if ((e = set_smem(unpack_oct64_tma_kernel<2>, sizeof(Oct64Smem<2>))) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_oct64_tma_kernel<3>, sizeof(Oct64Smem<3>))) != cudaSuccess) return e;
+  c.oct64_ctas[0] = occupancy(unpack_oct64_tma_kernel<2>, kQThreads, sizeof(Oct64Smem<2>));
+  c.oct64_ctas[1] = occupancy(unpack_oct64_tma_kernel<3>, kQThreads, sizeof(Oct64Smem<3>));
   if ((e = set_smem(unpack_kernel<false>, unpack_smem(false))) != cudaSuccess) return e;
   if ((e = set_smem(unpack_kernel<true>, unpack_smem(true))) != cudaSuccess) return e;
   return cudaSuccess;
@@ -2464,6 +2701,17 @@ cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
     note_launch(1);
     return cudaGetLastError();
   }
+  const int sched64 = g_unpack64_schedule.load(std::memory_order_relaxed);
+  if (sched64 == 1 || sched64 == 2) {
+    const int64_t groups = (a.n_blocks + 3) / 4;
+    int64_t grid = (int64_t)c->sms * unpack_ctas(c->oct64_ctas[sched64 - 1]);
+    const int64_t need = (groups + kQWarps - 1) / kQWarps;
+    if (grid > need) grid = need;
+    if (sched64 == 1) unpack_oct64_tma_kernel<2><<<(unsigned)grid, kQThreads, sizeof(Oct64Smem<2>), st>>>(a);
+    else unpack_oct64_tma_kernel<3><<<(unsigned)grid, kQThreads, sizeof(Oct64Smem<3>), st>>>(a);
+    note_launch(1);
+    return cudaGetLastError();
+  }
   const int64_t grid = tiles_for(a.n_blocks);
   unpack_kernel<true><<<(unsigned)grid, kThreads, unpack_smem(true), st>>>(a);
   note_launch(1);
@@ -2520,6 +2768,10 @@ int set_knob(int knob, int value) {
       if (value < 0 || value > 32) return -1;
       g_unpack_cap.store(value, std::memory_order_relaxed);
       return 0;
+    case 8:  // UTL_KNOB_UNPACK64_SCHEDULE
+      if (value < 0 || value > 2) return -1;
+      g_unpack64_schedule.store(value, std::memory_order_relaxed);
+      return 0;
     case 6:  // UTL_KNOB_PACK_WINDOW
       if (value < 0 || value > 2) return -1;
       g_pack_window.store(value, std::memory_order_relaxed);
@@ -2544,6 +2796,7 @@ int get_knob(int knob) {
     case 5: return g_keep_scratch.load(std::memory_order_relaxed);
     case 6: return g_pack_window.load(std::memory_order_relaxed);
     case 7: return g_unpack_cap.load(std::memory_order_relaxed);
+    case 8: return g_unpack64_schedule.load(std::memory_order_relaxed);
   }
   return -1;
 }

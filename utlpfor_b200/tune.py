@@ -16,9 +16,9 @@ that file (if any) for the current GPU and sets the knobs.  Knobs
                                  in flight per warp)
   7 UTL_KNOB_UNPACK_CTAS_PER_SM  warps per SM of the unpack (4 per CTA):
                                  0 occupancy maximum, else a cap
-The pack schedule and window are swept jointly, then the CTA cap of the
-winner; every pack candidate must give the same bytes, every unpack
-candidate the same values.
+The pack schedule (with the window left to its per-batch choice) is swept
+first, then the CTA cap of the winner; every pack candidate must give the
+same bytes, every unpack candidate the same values.
 
     python -m utlpfor_b200.tune [--log2n 26] [--out PATH]
 """
@@ -31,9 +31,13 @@ from ._lib import load
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 TUNED = os.path.join(HERE, "tuned")
-PACK_SHAPES = [(2, 2), (2, 1), (1, 2), (1, 1), (0, 1)]  # (schedule, window)
+# Candidates are the settings that suit any batch: the window and the
+# unpack staging size stay chosen per batch (window 0, unpack schedules 1
+# and 4 pick by block density), so a setting tuned on one workload cannot
+# slow down a batch of much larger blocks.
+PACK_SHAPES = [(1, 0), (2, 0), (0, 0)]  # (schedule, window)
 PACK_CAPS = [0, 16, 12, 8]
-UNPACK_SCHEDULES = [4, 5, 6, 1, 2, 3, 0]
+UNPACK_SCHEDULES = [1, 4, 0]
 UNPACK_CAPS = [0, 4, 3, 2]
 KNOBS = ("0", "1", "2", "6", "7")
 
