@@ -1060,7 +1060,9 @@ __device__ __forceinline__ void oct64_block(const SmemBytes& sb, int blk, int le
     status = st;
     ovf = ov;
     if (st != kOK || qh != 0) return;
-    if (want == kBlock) {
+    // 16-byte stores only where the output is 16-byte aligned (a stream may
+    // start at any value index)
+    if (want == kBlock && ((uintptr_t)op & 15) == 0) {
 #pragma unroll
       for (int v = 0; v < 8; v++) {
         const int i = 16 * v + 4 * j;
@@ -1107,7 +1109,7 @@ __device__ __forceinline__ void oct64_block(const SmemBytes& sb, int blk, int le
     const uint64_t v0 = qh == 0 ? ((uint64_t)a0 << 32 | x[v][0]) : ((uint64_t)x[v][2] << 32 | a0);
     const uint64_t v1 = qh == 0 ? ((uint64_t)a1 << 32 | x[v][1]) : ((uint64_t)x[v][3] << 32 | a1);
     const int i = 16 * v + 4 * j + i0;
-    if (want == kBlock) {
+    if (want == kBlock && ((uintptr_t)op & 15) == 0) {
       __stcs((ulonglong2*)(op + i), make_ulonglong2(v0, v1));
     } else {
       if (i < want) op[i] = v0;
