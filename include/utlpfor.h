@@ -309,10 +309,12 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *     1 = 3 or 2 by the batch's mean block length, decided on the device
  *     (the default);
  *     5 = persistent warps staging each group of 8 blocks with one TMA bulk
- *     copy, three groups in flight, up to 264 bytes a block, with the
- *     register fast path for blocks of at most 16 exceptions; 6 = the same
+ *     copy, three groups in flight, up to 264 bytes a block; 6 = the same
  *     with two groups of up to 528 bytes a block in flight; 4 = 5 or 6 by
- *     the batch's mean block length, decided on the device.
+ *     the batch's mean block length, decided on the device; 7 = 5 with a
+ *     register fast path for blocks of at most 16 exceptions (positions
+ *     turned into a bitmask, high bits ORed by rank, no shared-memory round
+ *     trip of the values).
  *   UTL_KNOB_PACK_CTAS_PER_SM: cap on resident pack CTAs per SM (0 = the
  *     occupancy maximum).
  *   UTL_KNOB_PACK_SCHEDULE: uint32 pack kernel, 0 = four threads per block
@@ -328,9 +330,9 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *     of the persistent unpack kernels, schedules 1-6 (0 = the occupancy
  *     maximum).
  *   UTL_KNOB_UNPACK64_SCHEDULE: the uint64 unpack kernel, 0 = a warp per
- *     block; 1 = an octet of lanes per block (one quad per uint32
- *     sub-block, both decoded at once), 4 blocks per warp staged by TMA bulk
- *     copies, two groups in flight (the default); 2 = the same with three.
+ *     block (the default); 1 = an octet of lanes per block (one quad per
+ *     uint32 sub-block, both decoded at once), 4 blocks per warp staged by
+ *     TMA bulk copies, two groups in flight; 2 = the same with three.
  *   UTL_KNOB_HOST_PIPELINE: the host-buffer batch calls, 0 = one pass
  *     (all copies in, kernels, all copies out); 1 = batches of 64 MiB of
  *     values or more are cut at block boundaries into pieces of

@@ -28,7 +28,8 @@ LENS = [1, 128, 300, 0, 257, 1000, 5, 129, 0, 4096, 77]
 
 
 UNPACK_SCHEDULES = {0: "unpack_tiles", 1: "unpack_pipelined", 2: "unpack_pipelined_wide",
-                    3: "unpack_pipelined_narrow", 4: "unpack_tma", 5: "unpack_tma_narrow", 6: "unpack_tma_wide"}
+                    3: "unpack_pipelined_narrow", 4: "unpack_tma", 5: "unpack_tma_narrow", 6: "unpack_tma_wide",
+                    7: "unpack_tma_fast"}
 
 
 @pytest.fixture(params=sorted(UNPACK_SCHEDULES), ids=[UNPACK_SCHEDULES[k] for k in sorted(UNPACK_SCHEDULES)])
@@ -39,6 +40,16 @@ def sched(request):
     assert L.utl_set_knob(0, request.param) == 0
     yield request.param
     L.utl_set_knob(0, old)
+
+
+@pytest.fixture(params=[0, 1], ids=["unpack64_warp", "unpack64_octet"])
+def u64sched(request):
+    from utlpfor_b200._lib import load
+    L = load()
+    old = L.utl_get_knob(8)
+    assert L.utl_set_knob(8, request.param) == 0
+    yield request.param
+    L.utl_set_knob(8, old)
 
 
 @pytest.fixture(params=[0, 1, 2], ids=["pack_quad", "pack_lane", "pack_pair"])
@@ -96,7 +107,7 @@ def _batch_u32_case(env, flag, kind, all_unpack=False):
 
 @pytest.mark.parametrize("flag", list(range(16)) + [16 | 5, 32 | 9, 48 | 15])
 @pytest.mark.parametrize("kind", ["for64", "full", "walk", "fit32", "upper_for", "zero"])
-def test_pack_unpack_batch_u64(env, flag, kind, psched):
+def test_pack_unpack_batch_u64(env, flag, kind, psched, u64sched):
     U, torch = env
     rng = np.random.default_rng(500 + flag)
     vals, vo = streams(rng, LENS, kind, is64=True)
@@ -182,7 +193,7 @@ def test_unpack_batch_corrupt_blocks(env, sched):
 
 
 @pytest.mark.parametrize("flag", [0, 1])
-def test_unpack_batch_corrupt_blocks_u64(env, sched, flag):
+def test_unpack_batch_corrupt_blocks_u64(env, u64sched, flag):
     """uint64 blocks (two-block and FOR64 shapes) with a damaged byte fail
     their own status with the reference's error class; the others decode."""
     U, torch = env
@@ -251,7 +262,7 @@ def test_large_round_trip_properties(env, sched, psched):
 
 
 @pytest.mark.parametrize("flag", [0, 1, 3, 4])
-def test_large_u64_mix(env, flag, psched):
+def test_large_u64_mix(env, flag, psched, u64sched):
     """2^21 uint64 values over 96 ragged streams mixing the three uint64
     shapes (FOR64, two-block, delta walk): the pack is byte-identical to the
     oracle under both pack schedules and the unpack restores every value."""

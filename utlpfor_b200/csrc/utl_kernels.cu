@@ -861,7 +861,7 @@ __device__ __forceinline__ bool stage_issue(const UnpackArgs& a, const TmaGroup&
   return false;
 }
 
-template <int STAGE, int NSTAGE, bool AUTO>
+template <int STAGE, int NSTAGE, bool AUTO, bool FAST>
 __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_tma_kernel(UnpackArgs a) {
   extern __shared__ uint4 smem4[];
   QuadTmaSmem<STAGE, NSTAGE>& S = *(QuadTmaSmem<STAGE, NSTAGE>*)smem4;
@@ -954,7 +954,7 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_tma_kernel(UnpackArg
           quad::QFast f;
           uint32_t x[8][4];
           quad::QResult r;
-          if (quad::fast_plan(sb, blk, len, j, qm, f)) r = quad::fast_decode(sb, blk, f, x, patch, j, qm);
+          if (FAST && quad::fast_plan(sb, blk, len, j, qm, f)) r = quad::fast_decode(sb, blk, f, x, patch, j, qm);
           else r = quad::quad_unpack_block(sb, blk, len, false, x, patch, j, qm);
           status = r.status;
           ovf = r.ovf;
@@ -2490,7 +2490,7 @@ cudaError_t stream_offsets(const uint64_t* block_off, const uint64_t* bstart, in
 
 // UTL_KNOB_UNPACK64_SCHEDULE: 0 = warp per block, 1 / 2 = an octet per
 // block with TMA staging, two / three groups in flight per warp.
-static std::atomic<int> g_unpack64_schedule{1};
+static std::atomic<int> g_unpack64_schedule{0};
 // UTL_KNOB_UNPACK_CTAS_PER_SM: cap on resident unpack CTAs (of 4 warps) per
 // SM of the persistent unpack kernels (0 = the occupancy maximum).
 static std::atomic<int> g_unpack_cap{0};
@@ -2510,14 +2510,14 @@ static cudaError_t unpack_pipe(const UnpackArgs& a, cudaStream_t st, int ctas) {
   note_launch(1);
   return cudaGetLastError();
 }
-template <int STAGE, int NSTAGE, bool AUTO>
+template <int STAGE, int NSTAGE, bool AUTO, bool FAST = false>
 static cudaError_t unpack_tma(const UnpackArgs& a, cudaStream_t st, int ctas) {
   const size_t smem = sizeof(QuadTmaSmem<STAGE, NSTAGE>);
   const int64_t groups = (a.n_blocks + 7) / 8;
   int64_t grid = (int64_t)num_sms() * unpack_ctas(ctas);
   const int64_t need = (groups + kQWarps - 1) / kQWarps;
   if (grid > need) grid = need;
-  unpack_quad_tma_kernel<STAGE, NSTAGE, AUTO><<<(unsigned)grid, kQThreads, smem, st>>>(a);
+  unpack_quad_tma_kernel<STAGE, NSTAGE, AUTO, FAST><<<(unsigned)grid, kQThreads, smem, st>>>(a);
   note_launch(1);
   return cudaGetLastError();
 }
@@ -2580,12 +2580,13 @@ static cudaError_t setup_device(int dev, DevCfg& c) {
   c.pipe_ctas = occupancy(unpack_quad_pipe_kernel<kPStageNarrow, false>, kQThreads, pn);
   c.pipe_wide_ctas = occupancy(unpack_quad_pipe_kernel<kPStageWide, false>, kQThreads, pw);
   const size_t tn = sizeof(QuadTmaSmem<kPStageNarrow, 3>), tw = sizeof(QuadTmaSmem<kPStageWide, 2>);
-  if ((e = set_smem(unpack_quad_tma_kernel<kPStageNarrow, 3, true>, tn)) != cudaSuccess) return e;
-  if ((e = set_smem(unpack_quad_tma_kernel<kPStageNarrow, 3, false>, tn)) != cudaSuccess) return e;
-  if ((e = set_smem(unpack_quad_tma_kernel<kPStageWide, 2, true>, tw)) != cudaSuccess) return e;
-  if ((e = set_smem(unpack_quad_tma_kernel<kPStageWide, 2, false>, tw)) != cudaSuccess) return e;
-  c.tma_ctas = occupancy(unpack_quad_tma_kernel<kPStageNarrow, 3, false>, kQThreads, tn);
-  c.tma_wide_ctas = occupancy(unpack_quad_tma_kernel<kPStageWide, 2, false>, kQThreads, tw);
+  if ((e = set_smem(unpack_quad_tma_kernel<kPStageNarrow, 3, true, false>, tn)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_tma_kernel<kPStageNarrow, 3, false, false>, tn)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_tma_kernel<kPStageWide, 2, true, false>, tw)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_tma_kernel<kPStageWide, 2, false, false>, tw)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_tma_kernel<kPStageNarrow, 3, false, true>, tn)) != cudaSuccess) return e;
+  c.tma_ctas = occupancy(unpack_quad_tma_kernel<kPStageNarrow, 3, false, false>, kQThreads, tn);
+  c.tma_wide_ctas = occupancy(unpack_quad_tma_kernel<kPStageWide, 2, false, false>, kQThreads, tw);
   if ((e = set_smem(unpack_oct64_tma_kernel<2>, sizeof(Oct64Smem<2>))) != cudaSuccess) return e;
   if ((e = set_smem(unpack_oct64_tma_kernel<3>, sizeof(Oct64Smem<3>))) != cudaSuccess) return e;
   c.oct64_ctas[0] = occupancy(unpack_oct64_tma_kernel<2>, kQThreads, sizeof(Oct64Smem<2>));
@@ -2696,6 +2697,7 @@ cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
     }
     if (g_unpack_schedule == 5) return unpack_tma<kPStageNarrow, 3, false>(a, st, c->tma_ctas);
     if (g_unpack_schedule == 6) return unpack_tma<kPStageWide, 2, false>(a, st, c->tma_wide_ctas);
+    if (g_unpack_schedule == 7) return unpack_tma<kPStageNarrow, 3, false, true>(a, st, c->tma_ctas);
     if (g_unpack_schedule == 2) return unpack_pipe<kPStageWide, false>(a, st, c->pipe_wide_ctas);
     if (g_unpack_schedule == 3) return unpack_pipe<kPStageNarrow, false>(a, st, c->pipe_ctas);
     const int64_t grid = (a.n_blocks + kQTile - 1) / kQTile;
@@ -2755,7 +2757,7 @@ cudaError_t plain_get(bool u64, int pos, const uint8_t* src, int64_t staged, int
 int set_knob(int knob, int value) {
   switch (knob) {
     case 0:  // UTL_KNOB_UNPACK_SCHEDULE
-      if (value < 0 || value > 6) return -1;
+      if (value < 0 || value > 7) return -1;
       g_unpack_schedule = value;
       return 0;
     case 1:  // UTL_KNOB_PACK_CTAS_PER_SM (0 = occupancy maximum)
