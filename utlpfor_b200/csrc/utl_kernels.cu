@@ -1825,23 +1825,8 @@ __device__ __forceinline__ void lane_block_offsets(const PackArgs& a, int64_t ti
 
 template <bool DELTA>
 __device__ __forceinline__ void lane_write(const lane::Plan& p, const uint4* slot, uint8_t* o) {
-  uint32_t bm[4];
-  if (__any_sync(__activemask(), p.exc > 0)) lane::write_block<DELTA, true>(p, slot, o, bm);
-  else lane::write_block<DELTA, false>(p, slot, o, bm);
-}
-// Every lane of the warp (a block or not): payloads and bitmap-indexed
-// exceptions per thread, position-list exceptions by the whole warp.
-template <bool DELTA>
-__device__ __forceinline__ void lane_write_tile(const lane::Plan& p, bool has, const uint4* slot, const uint8_t* inb,
-                                                uint8_t* img, int off, int lane) {
-  uint32_t bm[4] = {0, 0, 0, 0};
-  if (__any_sync(kFull, has && p.exc > 0)) {
-    if (has) lane::write_block<DELTA, true, true>(p, slot, img + off, bm);
-    __syncwarp();
-    lane::warp_list_exceptions<DELTA>(p, has, inb, img, off, bm, lane);
-  } else if (has) {
-    lane::write_block<DELTA, false>(p, slot, img + off, bm);
-  }
+  if (__any_sync(__activemask(), p.exc > 0)) lane::write_block<DELTA, true>(p, slot, o);
+  else lane::write_block<DELTA, false>(p, slot, o);
 }
 
 template <bool DELTA, int SHAPE>
@@ -1870,7 +1855,7 @@ __global__ void __launch_bounds__(kLThreads, 8) pack_lane_kernel(PackArgs a) {
     if (cur >= 0) {
       lane_win_issue(sc, prev, cur, lane, win);
       if (n_rounds <= 1) {
-        lane_write_tile<DELTA>(p, n > 0, slot, inb, img, off, lane);
+        if (n > 0) lane_write<DELTA>(p, slot, img + off);
       } else {
         // a tile larger than the image: its offset first, then one window
         // of blocks at a time is written and streamed out

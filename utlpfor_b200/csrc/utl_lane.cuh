@@ -366,11 +366,8 @@ __device__ __forceinline__ void pack_group<16>(const uint32_t (&w)[8][4], uint32
 // base, the UTL payload (scalar.go:7-59: lane L's eight values packed LSB
 // first into bw/4 words, word w of lane L at byte 64w + 4L), then the
 // exception index and StreamVByte data (exceptions.go:138-186).
-// COOP: a position list (at most 16 exceptions) is left to the warp's
-// cooperative writer (warp_list_exceptions), which gets the exception bitmap
-// in bm_out; a bitmap-indexed block is written here as usual.
-template <bool DELTA, bool EXC, bool COOP = false>
-__device__ void write_block(const Plan& p, const uint4* s4, uint8_t* o, uint32_t (&bm_out)[4]) {
+template <bool DELTA, bool EXC>
+__device__ void write_block(const Plan& p, const uint4* s4, uint8_t* o) {
   put_bytes(o, p.header, 4);
   int m = 4;
   if (p.exc) {
@@ -417,9 +414,6 @@ __device__ void write_block(const Plan& p, const uint4* s4, uint8_t* o, uint32_t
       default: break;  // bw 0: no payload
     }
   }
-#pragma unroll
-  for (int q = 0; q < 4; q++) bm_out[q] = bm[q];
-  if (COOP && p.exc <= 16) return;
   if (EXC && p.exc) {
     const uint32_t* s = (const uint32_t*)s4;
     uint8_t* xi = pay + 16 * bw;
@@ -455,97 +449,6 @@ __device__ void write_block(const Plan& p, const uint4* s4, uint8_t* o, uint32_t
     }
     if ((rank & 3) && (rank >> 2) < nc) svb[rank >> 2] = (uint8_t)ctrl;
   }
-}
-
-// Set bits of m below position p, and the position of the r-th set bit.
-__device__ __forceinline__ int rank_below(const uint32_t (&m)[4], int p) {
-  const int q = p >> 5;
-  const uint32_t low = (1u << (p & 31)) - 1u;
-  int r = 0;
-#pragma unroll
-  for (int t = 0; t < 4; t++) r += t < q ? __popc(m[t]) : (t == q ? __popc(m[t] & low) : 0);
-  return r;
-}
-__device__ __forceinline__ int nth_bit(const uint32_t (&m)[4], int r) {
-  int q = 0;
-#pragma unroll
-  for (int t = 0; t < 3; t++) {
-    const int c = __popc(q == 0 ? m[0] : q == 1 ? m[1] : m[2]);
-    if (r >= c) {
-      r -= c;
-      q++;
-    }
-  }
-  const uint32_t w = q == 0 ? m[0] : q == 1 ? m[1] : q == 2 ? m[2] : m[3];
-  return 32 * q + (int)__fns(w, 0, r + 1);
-}
-
-// The position lists and StreamVByte high bits (exceptions.go:138-186) of
-// every block of the tile that has 1..16 exceptions, written by the whole
-// warp: the tile's exceptions are numbered block after block (a warp scan
-// of the counts) and lane l takes exceptions l, l+32, ...  For each, the
-// owning block (a binary search over the scan), its rank in the block, its
-// position (the rank-th set bit of the block's bitmap) and its high bits
-// (the work value at that position shifted by the width); the 2-bit length
-// codes of a block meet in its lane by a reduction over the lanes holding
-// that block's exceptions (the control bytes), and then every exception's
-// data offset is the control bytes' prefix.  The whole warp calls it; lane
-// k owns block k (slot inb + k*kSlot, block bytes at img + off).
-template <bool DELTA>
-__device__ __forceinline__ void warp_list_exceptions(const Plan& p, bool has, const uint8_t* inb, uint8_t* img,
-                                                     int off, const uint32_t (&bm)[4], int lane) {
-  const int E = (has && p.exc > 0 && p.exc <= 16) ? p.exc : 0;
-  const int incl = warp_incl_scan(E, lane);
-  const int total = __shfl_sync(kFull, incl, 31);
-  if (total == 0) return;
-  const int excl = incl - E;
-  const int xo = off + p.p_off + 16 * p.bw;  // this block's index bytes, in the image
-  const int svbo = xo + p.idx_sz;            // its StreamVByte bytes
-  const int nc = (E + 3) >> 2;
-  uint32_t cw = 0;
-  for (int pass = 0; pass < 2; pass++) {
-    for (int b0 = 0; b0 < total; b0 += 32) {
-      const int i = b0 + lane;
-      const bool act = i < total;
-      int k = 0;
-#pragma unroll
-      for (int st = 16; st; st >>= 1) {
-        const int e = __shfl_sync(kFull, excl, k + st);
-        if (e <= i) k += st;
-      }
-      const int r = i - __shfl_sync(kFull, excl, k);
-      uint32_t b[4];
-#pragma unroll
-      for (int q = 0; q < 4; q++) b[q] = __shfl_sync(kFull, bm[q], k);
-      const int bwk = __shfl_sync(kFull, p.bw, k);
-      const uint32_t basek = __shfl_sync(kFull, p.base, k);
-      const bool zzk = __shfl_sync(kFull, (int)p.zz, k) != 0;
-      const int pos = act ? nth_bit(b, r) : 0;
-      const uint32_t* sk = (const uint32_t*)(inb + k * kSlot);
-      const uint32_t hv = act ? (work_at<DELTA>(sk, pos, basek, zzk) >> bwk) : 0u;
-      const int l = svb_len_of(hv);
-      if (pass == 0) {
-        // the codes of block k, gathered in lane k
-        const unsigned grp = __match_any_sync(kFull, act ? k : -1);
-        const uint32_t part = __reduce_or_sync(grp, act ? (uint32_t)(l - 1) << (2 * r) : 0u);
-        const int first = excl - b0;
-        const bool mine = E > 0 && first < 32 && first + E > 0;
-        const uint32_t got = __shfl_sync(kFull, part, mine ? max(first, 0) : lane);
-        if (mine) cw |= got;
-      } else {
-        const uint32_t cwk = __shfl_sync(kFull, cw, k);
-        const int nck = __shfl_sync(kFull, nc, k);
-        const int xok = __shfl_sync(kFull, xo, k);
-        const int svbk = __shfl_sync(kFull, svbo, k);
-        if (act) {
-          img[xok + r] = (uint8_t)pos;
-          const int dd = nck + r + quad::sum2bit(cwk & ((1u << (2 * r)) - 1u));
-          put_bytes(img + svbk + dd, hv, l);
-        }
-      }
-    }
-  }
-  for (int c = 0; c < nc; c++) img[svbo + c] = (uint8_t)(cw >> (8 * c));
 }
 
 }  // namespace lane
