@@ -789,26 +789,36 @@ def main():
                 lat_u.append(t2 - t1)
         tot = sum(lat_p) + sum(lat_u)
         # the same calls from 8 host threads through a pool of 8 contexts
-        pool = U.CompressorPool(8)
+        # (raw C-ABI calls on buffers prepared per thread; ctypes releases
+        # the interpreter lock for the duration of each call)
+        pool = C.c_void_p()
+        assert L.utl_pool_new(8, C.byref(pool)) == 0
         n_thr = 8
         per = max(1, (hv_n // 128) // n_thr)
 
-        def pool_worker(k):
-            for i in range(k * per, (k + 1) * per):
-                blk = hv[128 * i:128 * i + 128]
-                pk = pool.PackUint32(flag, blk)
-                got, _ = pool.UnpackUint32(pk)
-                assert np.array_equal(got, blk)
+        def pool_worker(k, reps):
+            pb = np.zeros(L.utl_max_block_length32(flag), dtype=np.uint8)
+            po = np.zeros(128, dtype=np.uint32)
+            n_, c_, cs_, ov_ = C.c_size_t(0), C.c_int(0), C.c_size_t(0), C.c_int(0)
+            pbp = pb.ctypes.data_as(C.POINTER(C.c_uint8))
+            pop = po.ctypes.data_as(C.POINTER(C.c_uint32))
+            blocks = [hv[128 * i:128 * i + 128] for i in range(k * per, (k + 1) * per)]
+            ptrs = [bl.ctypes.data_as(C.POINTER(C.c_uint32)) for bl in blocks]
+            for _ in range(reps):
+                for bl, bp in zip(blocks, ptrs):
+                    assert L.utl_pool_pack_u32(pool, flag, bp, bl.size, pbp, pb.size, C.byref(n_)) == 0
+                    assert L.utl_pool_unpack_u32(pool, pbp, n_.value, pop, C.byref(c_), C.byref(cs_),
+                                                 C.byref(ov_)) == 0
 
-        pool_worker(0)  # warm every context
-        ths = [threading.Thread(target=pool_worker, args=(k,)) for k in range(n_thr)]
+        pool_worker(0, 1)  # warm the contexts
+        ths = [threading.Thread(target=pool_worker, args=(k, 1)) for k in range(n_thr)]
         tp0 = time.perf_counter()
         for t_ in ths:
             t_.start()
         for t_ in ths:
             t_.join()
         pool_s = time.perf_counter() - tp0
-        pool.close()
+        L.utl_pool_free(pool)
         plain = {"GBps": 2 * 4 * hv_n / tot / 1e9, "unit": "GB/s (round-trip uncompressed)", "blocks": hv_n // 128,
                  "pooled_8_threads_GBps": 2 * 4 * 128 * per * n_thr / pool_s / 1e9,
                  "pack_us_p50": 1e6 * float(np.median(lat_p)), "pack_us_p99": 1e6 * float(np.percentile(lat_p, 99)),
