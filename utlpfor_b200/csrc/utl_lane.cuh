@@ -168,7 +168,7 @@ __device__ __forceinline__ void raw_stats(const uint4* s4, uint32_t& mn, uint32_
   mx = 0u;
   E = 0u;
   O = 0u;
-#pragma unroll 2
+#pragma unroll 1
   for (int c8 = 0; c8 < 8; c8++) {
     uint4 t[4];
 #pragma unroll
@@ -388,6 +388,10 @@ __device__ void write_block(const Plan& p, const uint4* s4, uint8_t* o) {
   uint32_t* pw = (uint32_t*)(pay - d4);
   const int sh = 32 - 8 * d4;
   uint32_t bm[4] = {0, 0, 0, 0};
+  // rolled: a smaller loop body keeps the pack's hot code in the
+  // instruction cache (measured: c3 pack 0.575 -> 0.539 ms with the rolled
+  // statistics loop below)
+#pragma unroll 1
   for (int g = 0; g < 4; g++) {
     uint32_t w[8][4];
     bool borrow = false;
