@@ -14,6 +14,8 @@
 // Decisions and byte layout follow the Go reference github.com/Akron/utlpfor
 // exactly; each step cites the file:line it matches.
 #pragma once
+#include <type_traits>
+
 #include "utl_device.cuh"
 
 namespace utl {
@@ -81,6 +83,49 @@ __device__ __forceinline__ void load16<SmemBytes>(const SmemBytes& s, int64_t a,
   w[1] = __funnelshift_r(w1, w2, sh);
   w[2] = __funnelshift_r(w2, w3, sh);
   w[3] = __funnelshift_r(w3, w4, sh);
+}
+
+// UTL payload of one quad lane at a bit width known at compile time
+// (scalar.go:65-116): the lane's BW/4 words of UTL lanes 4j..4j+3 are the
+// 16-byte windows at pbase + 64i; all are loaded first, then every row is
+// cut out with constant shifts (a value straddling words i and i+1 joins
+// them), so the loop has no branches and no loads between its rows.
+template <int BW>
+__device__ __forceinline__ void utl_rows(const SmemBytes& sb, int pbase, uint32_t (&x)[8][4]) {
+  constexpr int NW = BW / 4;
+  uint32_t w[NW][4];
+#pragma unroll
+  for (int i = 0; i < NW; i++) load16(sb, pbase + 64 * i, w[i]);
+#pragma unroll
+  for (int v = 0; v < 8; v++) {
+    const int pos = v * BW, wi = pos >> 5, sh = pos & 31;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t val = w[wi][k] >> sh;
+      if (sh + BW > 32) val |= w[wi + 1][k] << (32 - sh);
+      if (BW < 32) val &= (1u << (BW & 31)) - 1u;
+      x[v][k] = val;
+    }
+  }
+}
+
+// The same for any width (multiple of 4, at most 32) of a staged block.
+__device__ __forceinline__ void utl_rows_any(const SmemBytes& sb, int pbase, int bw, uint32_t (&x)[8][4]) {
+  switch (bw) {
+    case 4: utl_rows<4>(sb, pbase, x); break;
+    case 8: utl_rows<8>(sb, pbase, x); break;
+    case 12: utl_rows<12>(sb, pbase, x); break;
+    case 16: utl_rows<16>(sb, pbase, x); break;
+    case 20: utl_rows<20>(sb, pbase, x); break;
+    case 24: utl_rows<24>(sb, pbase, x); break;
+    case 28: utl_rows<28>(sb, pbase, x); break;
+    case 32: utl_rows<32>(sb, pbase, x); break;
+    default:
+#pragma unroll
+      for (int v = 0; v < 8; v++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) x[v][k] = 0;
+  }
 }
 
 // Bitmap-mode high bits (more than 16 exceptions): lane j sizes control
@@ -175,7 +220,9 @@ __device__ QResult quad_unpack_block(const Src& sb, int64_t blk, int64_t avail, 
   // UTL payload (scalar.go:65-116): the four lanes 4j..4j+3 of a word
   // index w are 16 contiguous bytes at 64w + 16j; a value straddling two
   // words is joined with a funnel shift.
-  if (bw == 0) {
+  if constexpr (std::is_same<Src, SmemBytes>::value) {
+    utl_rows_any(sb, (int)blk + p_off + 16 * j, bw, x);
+  } else if (bw == 0) {
 #pragma unroll
     for (int v = 0; v < 8; v++)
 #pragma unroll
