@@ -42,7 +42,8 @@ def sched(request):
     L.utl_set_knob(0, old)
 
 
-@pytest.fixture(params=[0, 1], ids=["unpack64_warp", "unpack64_octet"])
+@pytest.fixture(params=[0, 1, 3, 4, 5],
+                ids=["unpack64_warp", "unpack64_octet", "unpack64_quad", "unpack64_quad_narrow", "unpack64_quad_wide"])
 def u64sched(request):
     from utlpfor_b200._lib import load
     L = load()

@@ -594,7 +594,7 @@ __device__ UnpackResult warp_unpack_block(const Src& sb, int64_t blk, int64_t av
       }
     }
 #pragma unroll
-    for (int k = 0; k < 4; k++) v[k] = (lane + 32 * k < count) ? rows[2 * k + hh] : v[k];
+    for (int k = 0; k < 4; k++) v[k] = (lane + 32 * k < count) ? (hh ? rows[2 * k + 1] : rows[2 * k]) : v[k];  // static indices: rows stays in registers
     if (!zz) {
       // ErrOverflow.Position: first wrap in v-major order = lowest index.
       int m = __reduce_min_sync(kFull, (unsigned)first);

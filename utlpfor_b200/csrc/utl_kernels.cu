@@ -666,10 +666,10 @@ __device__ __forceinline__ GroupInfo group_load(const UnpackArgs& a, int64_t g, 
 }
 
 // whether a group's contiguous bytes fit one staging buffer (warp-uniform)
-template <int STAGE>
+template <int STAGE, int MAXB = kMaxBlock32>
 __device__ __forceinline__ bool group_fits(const UnpackArgs& a, const GroupInfo& gi, int lane) {
   const uint64_t next = __shfl_down_sync(kFull, gi.off, 1);
-  const bool ok = lane >= gi.nb || (next >= gi.off && next - gi.off <= (uint64_t)kMaxBlock32 && next <= a.packed_len);
+  const bool ok = lane >= gi.nb || (next >= gi.off && next - gi.off <= (uint64_t)MAXB && next <= a.packed_len);
   const uint64_t o0 = __shfl_sync(kFull, gi.off, 0), o1 = __shfl_sync(kFull, gi.off, gi.nb);
   const int ph = (int)(((uintptr_t)a.packed + o0) & 15);
   return __all_sync(kFull, ok) && (int64_t)(o1 - o0) + ph + 16 <= STAGE;
@@ -677,19 +677,96 @@ __device__ __forceinline__ bool group_fits(const UnpackArgs& a, const GroupInfo&
 
 // Mean packed block length above which a batch takes the wide staging.
 constexpr uint64_t kWideMean = 240;
+// The uint64 staging: groups of 8 single-sub-block blocks (narrow, the
+// uint32 wide budget) or of 8 two-block pairs of up to 1056 bytes (wide).
+constexpr int kP64StageWide = 8 * 1056;
+constexpr uint64_t kWideMean64 = 500;
+
+// Decode and store uint64 block at staging offset blk (len bytes) by a quad
+// (unpackUint64Block, uint64.go:191-266): the first uint32 sub-block, then
+// for a two-block pair the upper-halves sub-block after it, both with the
+// quad decode; values are joined in registers and stored as 16-byte pairs
+// where the output allows.  status / ovf are quad-uniform; nothing is
+// stored for a block that fails.
+__device__ __forceinline__ void quad64_block(const SmemBytes& sb, int blk, int len, uint64_t* op, int want,
+                                             uint32_t* patch, int j, unsigned qm, int& status, int& ovf) {
+  status = kOK;
+  ovf = 0;
+  if (len < 4) { status = kErrInvalidBuffer; return; }
+  const uint32_t h = sb.u32(blk);
+  if (((h >> 13) & 3) != 3) { status = kErrUnsupportedType; return; }
+  const int forw = (int)((h >> 15) & 3);
+  const int exc = (int)(h >> 24);
+  const bool full = want == kBlock && ((uintptr_t)op & 15) == 0;
+  uint32_t xl[8][4];
+  if (!(h & kHdrCombine)) {
+    // FOR64 (8-byte base in front of the payload) or fit-32
+    uint64_t base = 0;
+    if (forw == 3) {
+      const int off = 4 + (exc > 0 ? 2 : 0);
+      if (len < off + 8) { status = kErrInvalidBuffer; return; }
+      base = sb.u64(blk + off);
+    }
+    const quad::QResult r = quad::quad_unpack_block(sb, blk, len, true, xl, patch, j, qm);
+    if (r.status != kOK) { status = r.status; ovf = r.ovf; return; }
+    if (r.count != want || r.consumed != len) { status = kErrCountMismatch; return; }
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+      const int i = 16 * v + 4 * j;
+      if (full) {
+        __stcs((ulonglong2*)(op + i), make_ulonglong2(base + xl[v][0], base + xl[v][1]));
+        __stcs((ulonglong2*)(op + i + 2), make_ulonglong2(base + xl[v][2], base + xl[v][3]));
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          if (i + k < want) op[i + k] = base + xl[v][k];
+      }
+    }
+    return;
+  }
+  // two-block pair: the reference's order of checks (uint64.go:226-262)
+  const quad::QResult r1 = quad::quad_unpack_block(sb, blk, len, true, xl, patch, j, qm);
+  if (r1.status != kOK) { status = r1.status; ovf = r1.ovf; return; }
+  const int meta = 4 + (exc > 0 ? 2 : 0) + ((1 << forw) >> 1) + 2;  // its block2Len field ends here
+  if (len < meta) { status = kErrInvalidBuffer; return; }
+  const int b2len = (int)sb.u16(blk + meta - 2);
+  if (r1.consumed + b2len > len) { status = kErrInvalidBuffer; return; }
+  uint32_t xh[8][4];
+  const quad::QResult r2 = quad::quad_unpack_block(sb, blk + r1.consumed, b2len, true, xh, patch, j, qm);
+  if (r2.status != kOK) { status = r2.status; ovf = r2.ovf; return; }
+  if (r2.count != r1.count) { status = kErrInvalidBuffer; return; }
+  if (r1.count != want || r1.consumed + b2len != len) { status = kErrCountMismatch; return; }
+#pragma unroll
+  for (int v = 0; v < 8; v++) {
+    const int i = 16 * v + 4 * j;
+    uint64_t y[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) y[k] = ((uint64_t)xh[v][k] << 32) | xl[v][k];
+    if (full) {
+      __stcs((ulonglong2*)(op + i), make_ulonglong2(y[0], y[1]));
+      __stcs((ulonglong2*)(op + i + 2), make_ulonglong2(y[2], y[3]));
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        if (i + k < want) op[i + k] = y[k];
+    }
+  }
+}
 
 // AUTO: the narrow and the wide instance are both launched; each works out
 // from the block offsets which of them the batch's mean block length calls
-// for, and the other returns at once (same inputs, same answer).
-template <int STAGE, bool AUTO>
-__global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackArgs a) {
+// for, and the other returns at once (same inputs, same answer).  U64: a
+// quad per uint64 block (quad64_block), everything else as for uint32.
+template <int STAGE, bool AUTO, bool U64 = false>
+__global__ void __launch_bounds__(kQThreads, U64 ? 4 : 5) unpack_quad_pipe_kernel(UnpackArgs a) {
   extern __shared__ uint4 smem4[];
   QuadPipeSmem<STAGE>& S = *(QuadPipeSmem<STAGE>*)smem4;
+  constexpr int kMaxB = U64 ? kMaxBlock64 : kMaxBlock32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (AUTO) {
     const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
-    const bool wide = span > kWideMean * (uint64_t)a.n_blocks;
-    if (wide != (STAGE == kPStageWide)) return;
+    const bool wide = span > (U64 ? kWideMean64 : kWideMean) * (uint64_t)a.n_blocks;
+    if (wide != (STAGE == (U64 ? kP64StageWide : kPStageWide))) return;
   }
   const int q = lane >> 2, j = lane & 3;
   const unsigned qm = quad::quad_mask(lane);
@@ -700,7 +777,7 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackAr
   uint32_t* patch = (uint32_t*)S.patch[warp][q];
 
   GroupInfo cur = group_load(a, g, lane);
-  bool cur_fits = group_fits<STAGE>(a, cur, lane);
+  bool cur_fits = group_fits<STAGE, kMaxB>(a, cur, lane);
   if (cur_fits)
     stage_bytes_async(S.stage[warp][0], a.packed, a.packed_len, __shfl_sync(kFull, cur.off, 0),
                       __shfl_sync(kFull, cur.off, cur.nb), lane);
@@ -709,7 +786,7 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackAr
   for (int it = 0; g < n_groups; it++, g += stride) {
     const int buf = it & 1;
     // put the next group in flight, and start loading the one after it
-    const bool nxt_fits = nxt.nb > 0 && group_fits<STAGE>(a, nxt, lane);
+    const bool nxt_fits = nxt.nb > 0 && group_fits<STAGE, kMaxB>(a, nxt, lane);
     if (nxt_fits)
       stage_bytes_async(S.stage[warp][buf ^ 1], a.packed, a.packed_len, __shfl_sync(kFull, nxt.off, 0),
                         __shfl_sync(kFull, nxt.off, nxt.nb), lane);
@@ -721,7 +798,7 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackAr
     const int nb = cur.nb;
     const uint64_t off0 = __shfl_sync(kFull, cur.off, 0);
     const uint64_t s = __shfl_sync(kFull, cur.off, q), e = __shfl_sync(kFull, cur.off, q + 1);
-    const bool bad = e < s || e - s > (uint64_t)kMaxBlock32 || e > a.packed_len;
+    const bool bad = e < s || e - s > (uint64_t)kMaxB || e > a.packed_len;
     const int64_t b = cur.b0 + q;
     const int s0 = __shfl_sync(kFull, cur.s0, 0);
     const int rounds = cur_fits ? 1 : nb;
@@ -732,7 +809,7 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackAr
         // one block per round, synchronously, through this group's buffer
         const uint64_t rs = __shfl_sync(kFull, cur.off, rd), re = __shfl_sync(kFull, cur.off, rd + 1);
         __syncwarp();
-        if (re >= rs && re - rs <= (uint64_t)kMaxBlock32 && re <= a.packed_len)
+        if (re >= rs && re - rs <= (uint64_t)kMaxB && re <= a.packed_len)
           stage_bytes(S.stage[warp][buf], a.packed, a.packed_len, rs, re, lane, 32);
         __syncwarp();
       }
@@ -747,22 +824,27 @@ __global__ void __launch_bounds__(kQThreads, 5) unpack_quad_pipe_kernel(UnpackAr
           const int len = (int)(e - s);
           const int blk = cur_fits ? (int)(((uintptr_t)a.packed + off0) & 15) + (int)(s - off0)
                                    : (int)(((uintptr_t)a.packed + s) & 15);
-          uint32_t x[8][4];
-          const quad::QResult r =
-              quad::quad_unpack_block(SmemBytes{(const uint32_t*)stg}, blk, len, false, x, patch, j, qm);
-          status = r.status;
-          ovf = r.ovf;
-          if (status == kOK && (r.count != want || r.consumed != len)) status = kErrCountMismatch;
-          if (status == kOK) {
-            uint32_t* op = (uint32_t*)a.values + first;
-            if (want == kBlock) {
-              quad::quad_store_full(op, x, patch, j, qm);
-            } else {
+          if constexpr (U64) {
+            quad64_block(SmemBytes{(const uint32_t*)stg}, blk, len, (uint64_t*)a.values + first, want, patch, j, qm,
+                         status, ovf);
+          } else {
+            uint32_t x[8][4];
+            const quad::QResult r =
+                quad::quad_unpack_block(SmemBytes{(const uint32_t*)stg}, blk, len, false, x, patch, j, qm);
+            status = r.status;
+            ovf = r.ovf;
+            if (status == kOK && (r.count != want || r.consumed != len)) status = kErrCountMismatch;
+            if (status == kOK) {
+              uint32_t* op = (uint32_t*)a.values + first;
+              if (want == kBlock) {
+                quad::quad_store_full(op, x, patch, j, qm);
+              } else {
 #pragma unroll
-              for (int v = 0; v < 8; v++)
+                for (int v = 0; v < 8; v++)
 #pragma unroll
-                for (int k = 0; k < 4; k++)
-                  if (16 * v + 4 * j + k < want) op[16 * v + 4 * j + k] = x[v][k];
+                  for (int k = 0; k < 4; k++)
+                    if (16 * v + 4 * j + k < want) op[16 * v + 4 * j + k] = x[v][k];
+              }
             }
           }
         }
@@ -2392,6 +2474,7 @@ struct DevCfg {
   int tma_ctas = 0;              // unpack_quad_tma_kernel, narrow staging (3 stages)
   int tma_wide_ctas = 0;         // unpack_quad_tma_kernel, wide staging (2 stages)
   int oct64_ctas[2] = {0, 0};    // unpack_oct64_tma_kernel, 2 / 3 stages
+  int pipe64_ctas[2] = {0, 0};   // unpack_quad_pipe_kernel for uint64, narrow / wide staging
   int pack_ctas[2] = {0, 0};     // pack_kernel<false/true>
   // Mapped pinned pair the uint32 lane pack's last block fills with the
   // batch's packed bytes and block count; the next allocating launch on
@@ -2499,14 +2582,14 @@ static int unpack_ctas(int occ) {
   return (cap > 0 && cap < occ) ? cap : occ;
 }
 
-template <int STAGE, bool AUTO>
+template <int STAGE, bool AUTO, bool U64 = false>
 static cudaError_t unpack_pipe(const UnpackArgs& a, cudaStream_t st, int ctas) {
   const size_t psmem = sizeof(QuadPipeSmem<STAGE>);
   const int64_t groups = (a.n_blocks + 7) / 8;
   int64_t grid = (int64_t)num_sms() * unpack_ctas(ctas);
   const int64_t need = (groups + kQWarps - 1) / kQWarps;
   if (grid > need) grid = need;
-  unpack_quad_pipe_kernel<STAGE, AUTO><<<(unsigned)grid, kQThreads, psmem, st>>>(a);
+  unpack_quad_pipe_kernel<STAGE, AUTO, U64><<<(unsigned)grid, kQThreads, psmem, st>>>(a);
   note_launch(1);
   return cudaGetLastError();
 }
@@ -2591,6 +2674,13 @@ static cudaError_t setup_device(int dev, DevCfg& c) {
   if ((e = set_smem(unpack_oct64_tma_kernel<3>, sizeof(Oct64Smem<3>))) != cudaSuccess) return e;
   c.oct64_ctas[0] = occupancy(unpack_oct64_tma_kernel<2>, kQThreads, sizeof(Oct64Smem<2>));
   c.oct64_ctas[1] = occupancy(unpack_oct64_tma_kernel<3>, kQThreads, sizeof(Oct64Smem<3>));
+  const size_t qn = sizeof(QuadPipeSmem<kPStageWide>), qw = sizeof(QuadPipeSmem<kP64StageWide>);
+  if ((e = set_smem(unpack_quad_pipe_kernel<kPStageWide, true, true>, qn)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, true, true>, qw)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_pipe_kernel<kPStageWide, false, true>, qn)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, false, true>, qw)) != cudaSuccess) return e;
+  c.pipe64_ctas[0] = occupancy(unpack_quad_pipe_kernel<kPStageWide, false, true>, kQThreads, qn);
+  c.pipe64_ctas[1] = occupancy(unpack_quad_pipe_kernel<kP64StageWide, false, true>, kQThreads, qw);
   if ((e = set_smem(unpack_kernel<false>, unpack_smem(false))) != cudaSuccess) return e;
   if ((e = set_smem(unpack_kernel<true>, unpack_smem(true))) != cudaSuccess) return e;
   return cudaSuccess;
@@ -2706,6 +2796,13 @@ cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
     return cudaGetLastError();
   }
   const int sched64 = g_unpack64_schedule.load(std::memory_order_relaxed);
+  if (sched64 == 3) {  // quad per block, staging by the batch's mean block length on the device
+    e = unpack_pipe<kPStageWide, true, true>(a, st, c->pipe64_ctas[0]);
+    if (e != cudaSuccess) return e;
+    return unpack_pipe<kP64StageWide, true, true>(a, st, c->pipe64_ctas[1]);
+  }
+  if (sched64 == 4) return unpack_pipe<kPStageWide, false, true>(a, st, c->pipe64_ctas[0]);
+  if (sched64 == 5) return unpack_pipe<kP64StageWide, false, true>(a, st, c->pipe64_ctas[1]);
   if (sched64 == 1 || sched64 == 2) {
     const int64_t groups = (a.n_blocks + 3) / 4;
     int64_t grid = (int64_t)c->sms * unpack_ctas(c->oct64_ctas[sched64 - 1]);
@@ -2773,7 +2870,7 @@ int set_knob(int knob, int value) {
       g_unpack_cap.store(value, std::memory_order_relaxed);
       return 0;
     case 8:  // UTL_KNOB_UNPACK64_SCHEDULE
-      if (value < 0 || value > 2) return -1;
+      if (value < 0 || value > 5) return -1;
       g_unpack64_schedule.store(value, std::memory_order_relaxed);
       return 0;
     case 6:  // UTL_KNOB_PACK_WINDOW

@@ -124,24 +124,29 @@ __device__ __forceinline__ void group_work(const uint4* s4, int g, uint32_t base
   }
 }
 
-// Bucket histogram of the work values (and the delta borrow flag).
+// Bucket histogram of the work values (and the delta borrow flag).  An
+// out-of-line routine returns its results by value: they come back in
+// registers, where reference parameters would put the caller's variables
+// in local memory.
+struct Hist {
+  uint32_t E, O;
+  bool borrow;
+};
 template <bool DELTA>
-__device__ __noinline__ void work_hist(const uint4* s4, uint32_t base, bool zz, uint32_t& E, uint32_t& O,
-                                       bool& borrow) {
-  E = 0;
-  O = 0;
-  borrow = false;
+__device__ __noinline__ Hist work_hist(const uint4* s4, uint32_t base, bool zz) {
+  Hist h{0u, 0u, false};
   for (int g = 0; g < 4; g++) {
     uint32_t w[8][4];
-    group_work<DELTA>(s4, g, base, zz, w, borrow);
+    group_work<DELTA>(s4, g, base, zz, w, h.borrow);
 #pragma unroll
     for (int rp = 0; rp < 4; rp++) {
       uint32_t a = 0;
 #pragma unroll
       for (int k = 0; k < 4; k++) a += nib(w[2 * rp][k]) + nib(w[2 * rp + 1][k]);
-      widen(a, E, O);
+      widen(a, h.E, h.O);
     }
   }
+  return h;
 }
 
 // Work value at block position pos (exception high bits).
@@ -238,12 +243,13 @@ __device__ Plan plan_block(uint4* s4, int n, int flag, uint32_t type_flags = kTy
   if (DELTA || use_for) {
     if (n < kBlock) fill_padding(s, n, base);
     if (DELTA || mx != mn) {
-      bool borrow;
-      work_hist<DELTA>(s4, base, false, E, O, borrow);
-      if (DELTA && borrow) {
+      Hist hs = work_hist<DELTA>(s4, base, false);
+      if (DELTA && hs.borrow) {
         zz = true;
-        work_hist<DELTA>(s4, base, true, E, O, borrow);
+        hs = work_hist<DELTA>(s4, base, true);
       }
+      E = hs.E;
+      O = hs.O;
     } else {
       E = O = 0;  // a constant block under FOR: every work value is zero
     }

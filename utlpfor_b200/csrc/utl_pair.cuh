@@ -131,11 +131,9 @@ __device__ __forceinline__ void raw_stats(const uint4* s4, int h, uint32_t& mn, 
 
 // Bucket counts of the thread's work values (and the delta borrow).
 template <bool DELTA>
-__device__ __noinline__ void work_hist(const uint4* s4, int h, uint32_t base, bool zz, uint32_t& E, uint32_t& O,
-                                       bool& borrow) {
-  E = 0;
-  O = 0;
-  borrow = false;
+__device__ __noinline__ lane::Hist work_hist(const uint4* s4, int h, uint32_t base, bool zz) {
+  uint32_t E = 0, O = 0;
+  bool borrow = false;
 #pragma unroll
   for (int gi = 0; gi < 2; gi++) {
     const int g = h + 2 * gi;
@@ -153,6 +151,7 @@ __device__ __noinline__ void work_hist(const uint4* s4, int h, uint32_t base, bo
       lane::widen(a, E, O);
     }
   }
+  return lane::Hist{E, O, borrow};
 }
 
 // The padding of a partial block (n < 128) holds values whose work values
@@ -219,15 +218,14 @@ __device__ lane::Plan plan_block(uint4* s4, int n, int flag, int h, unsigned pm)
       __syncwarp(pm);
     }
     if (DELTA || mx != mn) {
-      bool borrow;
-      work_hist<DELTA>(s4, h, base, false, E, O, borrow);
-      E = padd(E, pm);
-      O = padd(O, pm);
-      if (DELTA && por(borrow ? 1u : 0u, pm)) {
+      lane::Hist hs = work_hist<DELTA>(s4, h, base, false);
+      E = padd(hs.E, pm);
+      O = padd(hs.O, pm);
+      if (DELTA && por(hs.borrow ? 1u : 0u, pm)) {
         zz = true;
-        work_hist<DELTA>(s4, h, base, true, E, O, borrow);
-        E = padd(E, pm);
-        O = padd(O, pm);
+        hs = work_hist<DELTA>(s4, h, base, true);
+        E = padd(hs.E, pm);
+        O = padd(hs.O, pm);
       }
     } else {
       E = O = 0;  // a constant block under FOR: every work value is zero
