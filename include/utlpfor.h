@@ -330,13 +330,15 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *     of the persistent unpack kernels, schedules 1-6 (0 = the occupancy
  *     maximum).
  *   UTL_KNOB_UNPACK64_SCHEDULE: the uint64 unpack kernel, 0 = a warp per
- *     block (the default); 1 = an octet of lanes per block (one quad per
+ *     block; 1 = an octet of lanes per block (one quad per
  *     uint32 sub-block, both decoded at once), 4 blocks per warp staged by
  *     TMA bulk copies, two groups in flight; 2 = the same with three;
  *     3 = a quad of lanes per block (the two sub-blocks of a pair one after
  *     the other), 8 blocks per warp, cp.async double buffer sized by the
  *     batch's mean block length; 4 / 5 = the same with the small / large
- *     buffer always.
+ *     buffer always; 6 = the large budget in a single buffer per warp
+ *     (twice the resident warps); 7 = as 3 with the large budget single
+ *     buffered (the default).
  *   UTL_KNOB_HOST_PIPELINE: the host-buffer batch calls, 0 = one pass
  *     (all copies in, kernels, all copies out); 1 = batches of 64 MiB of
  *     values or more are cut at block boundaries into pieces of

@@ -42,8 +42,9 @@ def sched(request):
     L.utl_set_knob(0, old)
 
 
-@pytest.fixture(params=[0, 1, 3, 4, 5],
-                ids=["unpack64_warp", "unpack64_octet", "unpack64_quad", "unpack64_quad_narrow", "unpack64_quad_wide"])
+@pytest.fixture(params=[0, 1, 3, 4, 5, 6, 7],
+                ids=["unpack64_warp", "unpack64_octet", "unpack64_quad", "unpack64_quad_narrow", "unpack64_quad_wide",
+                     "unpack64_quad_wide1", "unpack64_quad_auto1"])
 def u64sched(request):
     from utlpfor_b200._lib import load
     L = load()

@@ -613,9 +613,9 @@ __global__ void __launch_bounds__(kQThreads) unpack_quad_kernel(UnpackArgs a) {
 // to 528 bytes (batches whose blocks are wide)
 constexpr int kPStageNarrow = 8 * 264;
 constexpr int kPStageWide = 8 * 528;
-template <int STAGE>
+template <int STAGE, int NBUF = 2>
 struct QuadPipeSmem {
-  uint4 stage[kQWarps][2][(STAGE + kQStagePad) / 16];
+  uint4 stage[kQWarps][NBUF][(STAGE + kQStagePad) / 16];
   uint4 patch[kQWarps][8][kBlock / 4 + 1];  // +16 B: quads start on different banks
 };
 
@@ -684,10 +684,12 @@ constexpr uint64_t kWideMean64 = 500;
 
 // Decode and store uint64 block at staging offset blk (len bytes) by a quad
 // (unpackUint64Block, uint64.go:191-266): the first uint32 sub-block, then
-// for a two-block pair the upper-halves sub-block after it, both with the
-// quad decode; values are joined in registers and stored as 16-byte pairs
-// where the output allows.  status / ovf are quad-uniform; nothing is
-// stored for a block that fails.
+// for a two-block pair the upper-halves sub-block after it, both through
+// one quad decode call in a rolled loop (one copy of the decoder in the
+// kernel: three inlined copies overflowed the instruction cache); values
+// are joined in registers and stored as 16-byte pairs where the output
+// allows.  status / ovf are quad-uniform; nothing is stored for a block
+// that fails.
 __device__ __forceinline__ void quad64_block(const SmemBytes& sb, int blk, int len, uint64_t* op, int want,
                                              uint32_t* patch, int j, unsigned qm, int& status, int& ovf) {
   status = kOK;
@@ -697,51 +699,51 @@ __device__ __forceinline__ void quad64_block(const SmemBytes& sb, int blk, int l
   if (((h >> 13) & 3) != 3) { status = kErrUnsupportedType; return; }
   const int forw = (int)((h >> 15) & 3);
   const int exc = (int)(h >> 24);
-  const bool full = want == kBlock && ((uintptr_t)op & 15) == 0;
-  uint32_t xl[8][4];
-  if (!(h & kHdrCombine)) {
-    // FOR64 (8-byte base in front of the payload) or fit-32
-    uint64_t base = 0;
-    if (forw == 3) {
-      const int off = 4 + (exc > 0 ? 2 : 0);
-      if (len < off + 8) { status = kErrInvalidBuffer; return; }
-      base = sb.u64(blk + off);
-    }
-    const quad::QResult r = quad::quad_unpack_block(sb, blk, len, true, xl, patch, j, qm);
-    if (r.status != kOK) { status = r.status; ovf = r.ovf; return; }
-    if (r.count != want || r.consumed != len) { status = kErrCountMismatch; return; }
-#pragma unroll
-    for (int v = 0; v < 8; v++) {
-      const int i = 16 * v + 4 * j;
-      if (full) {
-        __stcs((ulonglong2*)(op + i), make_ulonglong2(base + xl[v][0], base + xl[v][1]));
-        __stcs((ulonglong2*)(op + i + 2), make_ulonglong2(base + xl[v][2], base + xl[v][3]));
-      } else {
-#pragma unroll
-        for (int k = 0; k < 4; k++)
-          if (i + k < want) op[i + k] = base + xl[v][k];
-      }
-    }
-    return;
+  const bool two = (h & kHdrCombine) != 0;
+  // FOR64 (8-byte base in front of the payload) or fit-32: one sub-block
+  uint64_t base = 0;
+  if (!two && forw == 3) {
+    const int off = 4 + (exc > 0 ? 2 : 0);
+    if (len < off + 8) { status = kErrInvalidBuffer; return; }
+    base = sb.u64(blk + off);
   }
-  // two-block pair: the reference's order of checks (uint64.go:226-262)
-  const quad::QResult r1 = quad::quad_unpack_block(sb, blk, len, true, xl, patch, j, qm);
-  if (r1.status != kOK) { status = r1.status; ovf = r1.ovf; return; }
-  const int meta = 4 + (exc > 0 ? 2 : 0) + ((1 << forw) >> 1) + 2;  // its block2Len field ends here
-  if (len < meta) { status = kErrInvalidBuffer; return; }
-  const int b2len = (int)sb.u16(blk + meta - 2);
-  if (r1.consumed + b2len > len) { status = kErrInvalidBuffer; return; }
-  uint32_t xh[8][4];
-  const quad::QResult r2 = quad::quad_unpack_block(sb, blk + r1.consumed, b2len, true, xh, patch, j, qm);
-  if (r2.status != kOK) { status = r2.status; ovf = r2.ovf; return; }
-  if (r2.count != r1.count) { status = kErrInvalidBuffer; return; }
-  if (r1.count != want || r1.consumed + b2len != len) { status = kErrCountMismatch; return; }
+  uint32_t x[8][4], xl[8][4];
+  int sub = blk, avail = len, count = 0, c1 = 0;
+#pragma unroll 1
+  for (int part = 0; part < (two ? 2 : 1); part++) {
+    // the width-generic payload loop: the per-width copies of the payload
+    // code cost this kernel more in instruction-cache misses than they save
+    const quad::QResult r = quad::quad_unpack_block<SmemBytes, false>(sb, sub, avail, true, x, patch, j, qm);
+    if (r.status != kOK) { status = r.status; ovf = r.ovf; return; }
+    if (part == 0) {
+      count = r.count;
+      c1 = r.consumed;
+      if (two) {
+        // the reference's order of checks for a pair (uint64.go:226-262)
+        const int meta = 4 + (exc > 0 ? 2 : 0) + ((1 << forw) >> 1) + 2;  // its block2Len field ends here
+        if (len < meta) { status = kErrInvalidBuffer; return; }
+        const int b2len = (int)sb.u16(blk + meta - 2);
+        if (c1 + b2len > len) { status = kErrInvalidBuffer; return; }
+        sub = blk + c1;
+        avail = b2len;
+#pragma unroll
+        for (int v = 0; v < 8; v++)
+#pragma unroll
+          for (int k = 0; k < 4; k++) xl[v][k] = x[v][k];
+      }
+    } else {
+      if (r.count != count) { status = kErrInvalidBuffer; return; }
+      c1 += avail;
+    }
+  }
+  if (count != want || c1 != len) { status = kErrCountMismatch; return; }
+  const bool full = want == kBlock && ((uintptr_t)op & 15) == 0;
 #pragma unroll
   for (int v = 0; v < 8; v++) {
     const int i = 16 * v + 4 * j;
     uint64_t y[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++) y[k] = ((uint64_t)xh[v][k] << 32) | xl[v][k];
+    for (int k = 0; k < 4; k++) y[k] = two ? (((uint64_t)x[v][k] << 32) | xl[v][k]) : base + x[v][k];
     if (full) {
       __stcs((ulonglong2*)(op + i), make_ulonglong2(y[0], y[1]));
       __stcs((ulonglong2*)(op + i + 2), make_ulonglong2(y[2], y[3]));
@@ -757,10 +759,13 @@ __device__ __forceinline__ void quad64_block(const SmemBytes& sb, int blk, int l
 // from the block offsets which of them the batch's mean block length calls
 // for, and the other returns at once (same inputs, same answer).  U64: a
 // quad per uint64 block (quad64_block), everything else as for uint32.
-template <int STAGE, bool AUTO, bool U64 = false>
+// NBUF 1: one staging buffer per warp, filled and waited for at the top of
+// each group (twice the resident warps of the double buffer for the large
+// uint64 budget, which hides the wait instead).
+template <int STAGE, bool AUTO, bool U64 = false, int NBUF = 2>
 __global__ void __launch_bounds__(kQThreads, U64 ? 4 : 5) unpack_quad_pipe_kernel(UnpackArgs a) {
   extern __shared__ uint4 smem4[];
-  QuadPipeSmem<STAGE>& S = *(QuadPipeSmem<STAGE>*)smem4;
+  QuadPipeSmem<STAGE, NBUF>& S = *(QuadPipeSmem<STAGE, NBUF>*)smem4;
   constexpr int kMaxB = U64 ? kMaxBlock64 : kMaxBlock32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (AUTO) {
@@ -778,21 +783,34 @@ __global__ void __launch_bounds__(kQThreads, U64 ? 4 : 5) unpack_quad_pipe_kerne
 
   GroupInfo cur = group_load(a, g, lane);
   bool cur_fits = group_fits<STAGE, kMaxB>(a, cur, lane);
-  if (cur_fits)
-    stage_bytes_async(S.stage[warp][0], a.packed, a.packed_len, __shfl_sync(kFull, cur.off, 0),
-                      __shfl_sync(kFull, cur.off, cur.nb), lane);
-  cp_async_commit();
+  if (NBUF == 2) {
+    if (cur_fits)
+      stage_bytes_async(S.stage[warp][0], a.packed, a.packed_len, __shfl_sync(kFull, cur.off, 0),
+                        __shfl_sync(kFull, cur.off, cur.nb), lane);
+    cp_async_commit();
+  }
   GroupInfo nxt = group_load(a, g + stride, lane);
   for (int it = 0; g < n_groups; it++, g += stride) {
-    const int buf = it & 1;
-    // put the next group in flight, and start loading the one after it
-    const bool nxt_fits = nxt.nb > 0 && group_fits<STAGE, kMaxB>(a, nxt, lane);
-    if (nxt_fits)
-      stage_bytes_async(S.stage[warp][buf ^ 1], a.packed, a.packed_len, __shfl_sync(kFull, nxt.off, 0),
-                        __shfl_sync(kFull, nxt.off, nxt.nb), lane);
-    cp_async_commit();
-    const GroupInfo nn = group_load(a, g + 2 * stride, lane);
-    cp_async_wait1();
+    const int buf = NBUF == 2 ? (it & 1) : 0;
+    bool nxt_fits = false;
+    GroupInfo nn;
+    if constexpr (NBUF == 2) {
+      // put the next group in flight, and start loading the one after it
+      nxt_fits = nxt.nb > 0 && group_fits<STAGE, kMaxB>(a, nxt, lane);
+      if (nxt_fits)
+        stage_bytes_async(S.stage[warp][buf ^ 1], a.packed, a.packed_len, __shfl_sync(kFull, nxt.off, 0),
+                          __shfl_sync(kFull, nxt.off, nxt.nb), lane);
+      cp_async_commit();
+      nn = group_load(a, g + 2 * stride, lane);
+      cp_async_wait1();
+    } else {
+      // this group now; the next group's offsets are already loading
+      if (cur_fits)
+        stage_bytes_async(S.stage[warp][0], a.packed, a.packed_len, __shfl_sync(kFull, cur.off, 0),
+                          __shfl_sync(kFull, cur.off, cur.nb), lane);
+      cp_async_commit();
+      asm volatile("cp.async.wait_all;" ::: "memory");
+    }
     __syncwarp();
 
     const int nb = cur.nb;
@@ -855,9 +873,15 @@ __global__ void __launch_bounds__(kQThreads, U64 ? 4 : 5) unpack_quad_pipe_kerne
       }
     }
     __syncwarp();
-    cur = nxt;
-    cur_fits = nxt_fits;
-    nxt = nn;
+    if constexpr (NBUF == 2) {
+      cur = nxt;
+      cur_fits = nxt_fits;
+      nxt = nn;
+    } else {
+      cur = nxt;
+      cur_fits = cur.nb > 0 && group_fits<STAGE, kMaxB>(a, cur, lane);
+      nxt = group_load(a, g + 2 * stride, lane);
+    }
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
@@ -2474,7 +2498,7 @@ struct DevCfg {
   int tma_ctas = 0;              // unpack_quad_tma_kernel, narrow staging (3 stages)
   int tma_wide_ctas = 0;         // unpack_quad_tma_kernel, wide staging (2 stages)
   int oct64_ctas[2] = {0, 0};    // unpack_oct64_tma_kernel, 2 / 3 stages
-  int pipe64_ctas[2] = {0, 0};   // unpack_quad_pipe_kernel for uint64, narrow / wide staging
+  int pipe64_ctas[3] = {0, 0, 0};  // unpack_quad_pipe_kernel for uint64: narrow, wide, wide single buffer
   int pack_ctas[2] = {0, 0};     // pack_kernel<false/true>
   // Mapped pinned pair the uint32 lane pack's last block fills with the
   // batch's packed bytes and block count; the next allocating launch on
@@ -2572,8 +2596,11 @@ cudaError_t stream_offsets(const uint64_t* block_off, const uint64_t* bstart, in
 }
 
 // UTL_KNOB_UNPACK64_SCHEDULE: 0 = warp per block, 1 / 2 = an octet per
-// block with TMA staging, two / three groups in flight per warp.
-static std::atomic<int> g_unpack64_schedule{0};
+// block with TMA staging, two / three groups in flight per warp, 3-7 = a
+// quad per block through the cp.async pipeline (7, the default: double
+// buffered small budget or single large buffer by the batch's mean block
+// length).
+static std::atomic<int> g_unpack64_schedule{7};
 // UTL_KNOB_UNPACK_CTAS_PER_SM: cap on resident unpack CTAs (of 4 warps) per
 // SM of the persistent unpack kernels (0 = the occupancy maximum).
 static std::atomic<int> g_unpack_cap{0};
@@ -2582,14 +2609,14 @@ static int unpack_ctas(int occ) {
   return (cap > 0 && cap < occ) ? cap : occ;
 }
 
-template <int STAGE, bool AUTO, bool U64 = false>
+template <int STAGE, bool AUTO, bool U64 = false, int NBUF = 2>
 static cudaError_t unpack_pipe(const UnpackArgs& a, cudaStream_t st, int ctas) {
-  const size_t psmem = sizeof(QuadPipeSmem<STAGE>);
+  const size_t psmem = sizeof(QuadPipeSmem<STAGE, NBUF>);
   const int64_t groups = (a.n_blocks + 7) / 8;
   int64_t grid = (int64_t)num_sms() * unpack_ctas(ctas);
   const int64_t need = (groups + kQWarps - 1) / kQWarps;
   if (grid > need) grid = need;
-  unpack_quad_pipe_kernel<STAGE, AUTO, U64><<<(unsigned)grid, kQThreads, psmem, st>>>(a);
+  unpack_quad_pipe_kernel<STAGE, AUTO, U64, NBUF><<<(unsigned)grid, kQThreads, psmem, st>>>(a);
   note_launch(1);
   return cudaGetLastError();
 }
@@ -2681,6 +2708,10 @@ static cudaError_t setup_device(int dev, DevCfg& c) {
   if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, false, true>, qw)) != cudaSuccess) return e;
   c.pipe64_ctas[0] = occupancy(unpack_quad_pipe_kernel<kPStageWide, false, true>, kQThreads, qn);
   c.pipe64_ctas[1] = occupancy(unpack_quad_pipe_kernel<kP64StageWide, false, true>, kQThreads, qw);
+  const size_t q1 = sizeof(QuadPipeSmem<kP64StageWide, 1>);
+  if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, true, true, 1>, q1)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, false, true, 1>, q1)) != cudaSuccess) return e;
+  c.pipe64_ctas[2] = occupancy(unpack_quad_pipe_kernel<kP64StageWide, false, true, 1>, kQThreads, q1);
   if ((e = set_smem(unpack_kernel<false>, unpack_smem(false))) != cudaSuccess) return e;
   if ((e = set_smem(unpack_kernel<true>, unpack_smem(true))) != cudaSuccess) return e;
   return cudaSuccess;
@@ -2803,6 +2834,12 @@ cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
   }
   if (sched64 == 4) return unpack_pipe<kPStageWide, false, true>(a, st, c->pipe64_ctas[0]);
   if (sched64 == 5) return unpack_pipe<kP64StageWide, false, true>(a, st, c->pipe64_ctas[1]);
+  if (sched64 == 6) return unpack_pipe<kP64StageWide, false, true, 1>(a, st, c->pipe64_ctas[2]);
+  if (sched64 == 7) {  // as 3, the large budget with a single buffer
+    e = unpack_pipe<kPStageWide, true, true>(a, st, c->pipe64_ctas[0]);
+    if (e != cudaSuccess) return e;
+    return unpack_pipe<kP64StageWide, true, true, 1>(a, st, c->pipe64_ctas[2]);
+  }
   if (sched64 == 1 || sched64 == 2) {
     const int64_t groups = (a.n_blocks + 3) / 4;
     int64_t grid = (int64_t)c->sms * unpack_ctas(c->oct64_ctas[sched64 - 1]);
@@ -2870,7 +2907,7 @@ int set_knob(int knob, int value) {
       g_unpack_cap.store(value, std::memory_order_relaxed);
       return 0;
     case 8:  // UTL_KNOB_UNPACK64_SCHEDULE
-      if (value < 0 || value > 5) return -1;
+      if (value < 0 || value > 7) return -1;
       g_unpack64_schedule.store(value, std::memory_order_relaxed);
       return 0;
     case 6:  // UTL_KNOB_PACK_WINDOW

@@ -171,7 +171,7 @@ __device__ __forceinline__ bool decode_bitmap_high_bits(const Src& sb, int64_t s
 // decodeUnpackHeader unpack_block.go:62-172 and applyExceptions
 // exceptions.go:194-284).  x[v][c] receives position 16v+4j+c.  patch is
 // the quad's 128-word shared scratch.  Results are quad-uniform.
-template <class Src>
+template <class Src, bool WIDTH_SPEC = true>
 __device__ QResult quad_unpack_block(const Src& sb, int64_t blk, int64_t avail, bool for_u64, uint32_t (&x)[8][4],
                                      uint32_t* patch, int j, unsigned qm) {
   QResult r{kOK, 0, 0, 0};
@@ -220,7 +220,7 @@ __device__ QResult quad_unpack_block(const Src& sb, int64_t blk, int64_t avail, 
   // UTL payload (scalar.go:65-116): the four lanes 4j..4j+3 of a word
   // index w are 16 contiguous bytes at 64w + 16j; a value straddling two
   // words is joined with a funnel shift.
-  if constexpr (std::is_same<Src, SmemBytes>::value) {
+  if constexpr (std::is_same<Src, SmemBytes>::value && WIDTH_SPEC) {
     utl_rows_any(sb, (int)blk + p_off + 16 * j, bw, x);
   } else if (bw == 0) {
 #pragma unroll
