@@ -314,7 +314,11 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *     the batch's mean block length, decided on the device; 7 = 5 with a
  *     register fast path for blocks of at most 16 exceptions (positions
  *     turned into a bitmask, high bits ORed by rank, no shared-memory round
- *     trip of the values).
+ *     trip of the values); 9 = one thread per block (tiles of 32 blocks per
+ *     warp, rows written out through a shared-memory chunk), the quad decoder
+ *     for blocks it does not take (bitmap exceptions, plain delta, partial,
+ *     corrupt or oversized blocks); 8 = 9 for batches of at most 200 bytes a
+ *     block on average, else as 1, decided on the device.
  *   UTL_KNOB_PACK_CTAS_PER_SM: cap on resident pack CTAs per SM (0 = the
  *     occupancy maximum).
  *   UTL_KNOB_PACK_SCHEDULE: uint32 pack kernel, 0 = four threads per block

@@ -11,7 +11,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libutlpfor_b200.so")
 SOURCES = ["utl_kernels.cu", "utl_capi.cu", "utl_noalloc.cu", "utl_index.cu"]
-HEADERS = ["utl_device.cuh", "utl_launch.h", "utl_quad.cuh", "utl_lane.cuh", "utl_pieces.h", "utl_unpack.cuh", "utl_pair.cuh"]
+HEADERS = ["utl_device.cuh", "utl_launch.h", "utl_quad.cuh", "utl_lane.cuh", "utl_pieces.h", "utl_unpack.cuh", "utl_pair.cuh",
+           "utl_unlane.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -24,6 +24,7 @@
 #include "utl_quad.cuh"
 #include "utl_unpack.cuh"
 #include "utl_pair.cuh"
+#include "utl_unlane.cuh"
 
 namespace utl {
 
@@ -772,6 +773,7 @@ __global__ void __launch_bounds__(kQThreads, U64 ? 4 : 5) unpack_quad_pipe_kerne
     const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
     const bool wide = span > (U64 ? kWideMean64 : kWideMean) * (uint64_t)a.n_blocks;
     if (wide != (STAGE == (U64 ? kP64StageWide : kPStageWide))) return;
+    if (!wide && span <= a.lane_mean * (uint64_t)a.n_blocks) return;
   }
   const int q = lane >> 2, j = lane & 3;
   const unsigned qm = quad::quad_mask(lane);
@@ -884,6 +886,230 @@ __global__ void __launch_bounds__(kQThreads, U64 ? 4 : 5) unpack_quad_pipe_kerne
     }
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// Thread-per-block uint32 unpack (utl_unlane.cuh): persistent warps over
+// tiles of 32 blocks.  AUTO: launched next to the two pipe instances; each
+// of the three works out from the block offsets whether the batch's mean
+// block length is its class, the other two return at once.
+constexpr int kLUStage = 32 * 264;   // a tile of 32 blocks of up to 264 bytes
+constexpr uint64_t kLaneMean = 200;  // mean packed block length up to which the thread path runs
+struct LaneUnpackSmem {
+  uint4 stage[kQWarps][(kLUStage + kQStagePad) / 16];
+  // the output chunk of the tile's 32 blocks; after the chunks, the quads'
+  // exception scratch of the fallback (8 x 132 words)
+  uint4 tile[kQWarps][32 * unlane::kTileStride / 16];
+};
+static_assert(32 * unlane::kTileStride >= 8 * (kBlock + 4) * 4, "fallback scratch");
+
+// The quad decoder on the blocks of `todo` (bit i: block b0 + i).  staged:
+// the tile's bytes are in stg with block i at ph + (s_i - s_0); otherwise
+// rounds of consecutive blocks that fit are staged here one after the
+// other.  Per-lane inputs are lane i's block values (s, e, first, want, ok).
+__device__ __forceinline__ void unlane_fallback(const UnpackArgs& a, uint4* stg, uint32_t* scratch, int64_t b0, int nb,
+                                             uint32_t todo, bool staged, int ph, uint64_t s, uint64_t e,
+                                             uint64_t first, int want, bool ok, int lane) {
+  const int q = lane >> 2, j = lane & 3;
+  const unsigned qm = quad::quad_mask(lane);
+  uint32_t* patch = scratch + q * (kBlock + 4);
+  const uint64_t s0 = __shfl_sync(kFull, s, 0);
+  int next = 0;  // unstaged mode: first block of the next round
+  while (staged ? todo != 0u : next < nb) {
+    // this round's blocks: quad q takes block bi (or none)
+    int bi = -1, rph = 0;
+    uint64_t rbase = 0;
+    if (staged) {
+      const int cnt = min(8, __popc(todo));
+      if (q < cnt) bi = (int)__fns(todo, 0, q + 1);
+      const uint32_t cut = cnt < __popc(todo) ? (uint32_t)__fns(todo, 0, 9) : 32u;
+      todo &= cut >= 32u ? 0u : ~((1u << cut) - 1u);
+      rph = ph;
+      rbase = s0;
+    } else {
+      // consecutive blocks from `next` whose bytes fit the buffer together
+      const uint64_t rs = __shfl_sync(kFull, s, next);
+      const int p0 = (int)(((uintptr_t)a.packed + rs) & 15);
+      const bool fit = lane >= next && lane < next + 8 && lane < nb && ok && e >= rs &&
+                       (int64_t)(e - rs) + p0 + 16 <= kLUStage;
+      const unsigned fm = __ballot_sync(kFull, fit) >> next;
+      const int cnt = max(1, __ffs(~fm) - 1);  // a bad first block is a round of its own
+      const bool any = (fm & 1u) != 0;
+      if (any) {
+        const uint64_t re = __shfl_sync(kFull, e, next + cnt - 1);
+        stage_bytes(stg, a.packed, a.packed_len, rs, re, lane, 32);
+      }
+      if (q < cnt) bi = next + q;
+      next += cnt;
+      rph = p0;
+      rbase = rs;
+      __syncwarp();
+    }
+    const int src = bi >= 0 ? bi : 0;
+    const uint64_t bs = __shfl_sync(kFull, s, src), be = __shfl_sync(kFull, e, src);
+    const uint64_t bf = __shfl_sync(kFull, first, src);
+    const int bw = __shfl_sync(kFull, want, src);
+    const bool bok = __shfl_sync(kFull, ok ? 1 : 0, src) != 0;
+    if (bi >= 0) {
+      int status = kOK, ovf = 0;
+      if (!bok) {
+        status = kErrCountMismatch;
+      } else {
+        const int len = (int)(be - bs);
+        const int blk = rph + (int)(bs - rbase);
+        uint32_t x[8][4];
+        const quad::QResult r = quad::quad_unpack_block(SmemBytes{(const uint32_t*)stg}, blk, len, false, x, patch, j, qm);
+        status = r.status;
+        ovf = r.ovf;
+        if (status == kOK && (r.count != bw || r.consumed != len)) status = kErrCountMismatch;
+        if (status == kOK) {
+          uint32_t* op = (uint32_t*)a.values + bf;
+          if (bw == kBlock) {
+            quad::quad_store_full(op, x, patch, j, qm);
+          } else {
+#pragma unroll
+            for (int v = 0; v < 8; v++)
+#pragma unroll
+              for (int k = 0; k < 4; k++)
+                if (16 * v + 4 * j + k < bw) op[16 * v + 4 * j + k] = x[v][k];
+          }
+        }
+      }
+      if (j == 0) {
+        if (a.block_status) a.block_status[b0 + bi] = status | (ovf << 8);
+        if (status != kOK && a.err) atomicOr(a.err, 1u << status);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <bool AUTO>
+__global__ void __launch_bounds__(kQThreads, 4) unpack_lane_kernel(UnpackArgs a) {
+  using namespace unlane;
+  extern __shared__ uint4 smem4[];
+  LaneUnpackSmem& S = *(LaneUnpackSmem*)smem4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (AUTO) {
+    const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
+    if (span > a.lane_mean * (uint64_t)a.n_blocks) return;
+  }
+  const int64_t n_tiles = (a.n_blocks + 31) / 32;
+  const int64_t stride = (int64_t)gridDim.x * kQWarps;
+  uint4* stg = S.stage[warp];
+  uint8_t* tileb = (uint8_t*)S.tile[warp];
+  uint8_t* T = tileb + lane * kTileStride;
+  const SmemBytes sb{(const uint32_t*)stg};
+  for (int64_t t = (int64_t)blockIdx.x * kQWarps + warp; t < n_tiles; t += stride) {
+    const int64_t b0 = t * 32;
+    const int nb = (int)min((int64_t)32, a.n_blocks - b0);
+    const bool mine = lane < nb;
+    const uint64_t s = mine ? a.block_off[b0 + lane] : 0ull;
+    const uint64_t e = mine ? a.block_off[b0 + lane + 1] : 0ull;
+    const bool ok = mine && e >= s && e - s <= (uint64_t)kMaxBlock32 && e <= a.packed_len;
+    const uint64_t o0 = __shfl_sync(kFull, s, 0), oN = __shfl_sync(kFull, e, nb - 1);
+    const int ph = (int)(((uintptr_t)a.packed + o0) & 15);
+    // contiguous and in bounds: every block's end is the next one's start
+    const uint64_t nxt_s = __shfl_down_sync(kFull, s, 1);
+    const bool chain = !mine || lane == nb - 1 || nxt_s == e;
+    const bool fits = __all_sync(kFull, !mine || (ok && chain)) && (int64_t)(oN - o0) + ph + 16 <= kLUStage;
+    // the values each block decodes to
+    const int s0 = __shfl_sync(kFull, lane == 0 ? stream_of(a.block_start, a.n_streams, b0) : 0, 0);
+    uint64_t first = 0;
+    int want = 0;
+    if (mine) span_in(a.val_off, a.block_start, stream_from(a.block_start, a.n_streams, s0, b0 + lane), b0 + lane,
+                      &first, &want);
+    if (fits) {
+      stage_bytes_async(stg, a.packed, a.packed_len, o0, oN, lane);
+      cp_async_commit();
+      asm volatile("cp.async.wait_all;" ::: "memory");
+    }
+    __syncwarp();
+    Plan f;
+    const bool fast = fits && mine && plan(sb, ph + (int)(s - o0), (int)(e - s), want, f);
+    const uint32_t fastm = __ballot_sync(kFull, fast);
+    if (fastm) {
+      uint32_t cur[16], nxt[16], acc[16];
+      int wi = 0, ex = 0, np = 256, doff = 0;
+#pragma unroll
+      for (int i = 0; i < 16; i++) cur[i] = nxt[i] = acc[i] = 0;
+      if (fast) {
+        if (f.bw > 0) load_words(sb, f.pay, cur);
+        if (f.bw > 4) load_words(sb, f.pay + 64, nxt);
+        if (f.exc > 0) np = (int)sb.u8(f.xo);
+        doff = f.nc;
+      }
+#pragma unroll 1
+      for (int c = 0; c < 8 / kRows; c++) {
+        if (fast) {
+#pragma unroll 1
+          for (int r = 0; r < kRows; r++) {
+            const int v = c * kRows + r;
+            const int sh = v * f.bw - 32 * wi;
+            uint32_t y[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) y[i] = __funnelshift_r(cur[i], nxt[i], sh) & f.mask;
+            if (f.delta) {
+              // zigzag delta (delta.go:50-115): the per-lane running sum
+#pragma unroll
+              for (int i = 0; i < 16; i++) {
+                acc[i] = (v == 0 ? 0u : acc[i]) + zz_dec(y[i]);
+                y[i] = acc[i];
+              }
+            }
+#pragma unroll
+            for (int i = 0; i < 16; i++) y[i] += f.base;
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+              *(uint4*)(T + 64 * r + 16 * i) = make_uint4(y[4 * i], y[4 * i + 1], y[4 * i + 2], y[4 * i + 3]);
+            if ((v + 1) * f.bw >= 32 * (wi + 1)) {
+#pragma unroll
+              for (int i = 0; i < 16; i++) cur[i] = nxt[i];
+              wi++;
+              if (4 * (wi + 1) < f.bw) load_words(sb, f.pay + 64 * (wi + 1), nxt);
+            }
+          }
+          // this chunk's exceptions (applyExceptions, exceptions.go:194-284):
+          // the high bits above the FOR-added low bits, in list order
+          while (np < 16 * kRows * (c + 1)) {
+            const int code = (int)((f.cw >> (2 * ex)) & 3);
+            uint32_t hv = sb.u32(f.svb + doff);
+            if (code < 3) hv &= (1u << (8 * (code + 1))) - 1u;
+            doff += code + 1;
+            uint32_t* tp = (uint32_t*)(T + 64 * ((np >> 4) - c * kRows) + 4 * (np & 15));
+            *tp = ((*tp - f.base) | shl32(hv, f.bw)) + f.base;
+            ex++;
+            np = ex < f.exc ? (int)sb.u8(f.xo + ex) : 256;
+          }
+        }
+        __syncwarp();
+        // the chunk's rows of every thread-path block, 16 bytes per lane
+        const int part = lane % kLanesPerBlock;
+#pragma unroll 1
+        for (int it = 0; it < 32 / kBlocksPerStore; it++) {
+          const int i = it * kBlocksPerStore + lane / kLanesPerBlock;
+          const uint64_t fi = __shfl_sync(kFull, first, i);
+          if ((fastm >> i) & 1u) {
+            const uint4 val = *(const uint4*)(tileb + i * kTileStride + 16 * part);
+            uint32_t* op = (uint32_t*)a.values + fi + 16 * kRows * c + 4 * part;
+            if ((fi & 3) == 0) {
+              __stcs((uint4*)op, val);
+            } else {
+              op[0] = val.x;
+              op[1] = val.y;
+              op[2] = val.z;
+              op[3] = val.w;
+            }
+          }
+        }
+        __syncwarp();
+      }
+      if (fast && a.block_status) a.block_status[b0 + lane] = kOK;
+    }
+    const uint32_t todo = __ballot_sync(kFull, mine && !fast);
+    if (todo)
+      unlane_fallback(a, stg, (uint32_t*)tileb, b0, nb, todo, fits, ph, s, e, first, want, ok, lane);
+    __syncwarp();
+  }
 }
 
 // TMA-staged pipelined unpack (utl_unpack.cuh): persistent warps over
@@ -2498,6 +2724,7 @@ struct DevCfg {
   int tma_ctas = 0;              // unpack_quad_tma_kernel, narrow staging (3 stages)
   int tma_wide_ctas = 0;         // unpack_quad_tma_kernel, wide staging (2 stages)
   int oct64_ctas[2] = {0, 0};    // unpack_oct64_tma_kernel, 2 / 3 stages
+  int lane_unpack_ctas = 0;       // unpack_lane_kernel
   int pipe64_ctas[3] = {0, 0, 0};  // unpack_quad_pipe_kernel for uint64: narrow, wide, wide single buffer
   int pack_ctas[2] = {0, 0};     // pack_kernel<false/true>
   // Mapped pinned pair the uint32 lane pack's last block fills with the
@@ -2620,6 +2847,16 @@ static cudaError_t unpack_pipe(const UnpackArgs& a, cudaStream_t st, int ctas) {
   note_launch(1);
   return cudaGetLastError();
 }
+template <bool AUTO>
+static cudaError_t unpack_lane(const UnpackArgs& a, cudaStream_t st, int ctas) {
+  const int64_t tiles = (a.n_blocks + 31) / 32;
+  int64_t grid = (int64_t)num_sms() * unpack_ctas(ctas);
+  const int64_t need = (tiles + kQWarps - 1) / kQWarps;
+  if (grid > need) grid = need;
+  unpack_lane_kernel<AUTO><<<(unsigned)grid, kQThreads, sizeof(LaneUnpackSmem), st>>>(a);
+  note_launch(1);
+  return cudaGetLastError();
+}
 template <int STAGE, int NSTAGE, bool AUTO, bool FAST = false>
 static cudaError_t unpack_tma(const UnpackArgs& a, cudaStream_t st, int ctas) {
   const size_t smem = sizeof(QuadTmaSmem<STAGE, NSTAGE>);
@@ -2708,6 +2945,9 @@ static cudaError_t setup_device(int dev, DevCfg& c) {
   if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, false, true>, qw)) != cudaSuccess) return e;
   c.pipe64_ctas[0] = occupancy(unpack_quad_pipe_kernel<kPStageWide, false, true>, kQThreads, qn);
   c.pipe64_ctas[1] = occupancy(unpack_quad_pipe_kernel<kP64StageWide, false, true>, kQThreads, qw);
+  if ((e = set_smem(unpack_lane_kernel<true>, sizeof(LaneUnpackSmem))) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_lane_kernel<false>, sizeof(LaneUnpackSmem))) != cudaSuccess) return e;
+  c.lane_unpack_ctas = occupancy(unpack_lane_kernel<false>, kQThreads, sizeof(LaneUnpackSmem));
   const size_t q1 = sizeof(QuadPipeSmem<kP64StageWide, 1>);
   if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, true, true, 1>, q1)) != cudaSuccess) return e;
   if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, false, true, 1>, q1)) != cudaSuccess) return e;
@@ -2806,6 +3046,16 @@ cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
   cudaError_t e = dev_cfg(&c);
   if (e != cudaSuccess) return e;
   if (!u64) {
+    if (g_unpack_schedule == 8) {  // thread per block for small blocks, else as 1; decided on the device
+      UnpackArgs b = a;
+      b.lane_mean = kLaneMean;
+      e = unpack_lane<true>(b, st, c->lane_unpack_ctas);
+      if (e != cudaSuccess) return e;
+      e = unpack_pipe<kPStageNarrow, true>(b, st, c->pipe_ctas);
+      if (e != cudaSuccess) return e;
+      return unpack_pipe<kPStageWide, true>(b, st, c->pipe_wide_ctas);
+    }
+    if (g_unpack_schedule == 9) return unpack_lane<false>(a, st, c->lane_unpack_ctas);
     if (g_unpack_schedule == 1) {  // by the batch's mean block length, decided on the device
       e = unpack_pipe<kPStageNarrow, true>(a, st, c->pipe_ctas);
       if (e != cudaSuccess) return e;
@@ -2891,7 +3141,7 @@ cudaError_t plain_get(bool u64, int pos, const uint8_t* src, int64_t staged, int
 int set_knob(int knob, int value) {
   switch (knob) {
     case 0:  // UTL_KNOB_UNPACK_SCHEDULE
-      if (value < 0 || value > 7) return -1;
+      if (value < 0 || value > 9) return -1;
       g_unpack_schedule = value;
       return 0;
     case 1:  // UTL_KNOB_PACK_CTAS_PER_SM (0 = occupancy maximum)

@@ -35,6 +35,8 @@ struct UnpackArgs {
   int32_t* block_status;
   uint32_t* err;
   uint32_t spin_limit = 1u << 22;  // polls of each bounded wait (UTL_KNOB_SPIN_LIMIT)
+  uint64_t lane_mean = 0;  // > 0: the small-staging pipe instance leaves batches of at most this mean block length
+                           // to the thread-per-block kernel launched beside it
 };
 
 struct GetArgs {
