@@ -649,12 +649,18 @@ def main():
     traffic = profiled_traffic()
     dom = "pack" if pack_ms >= unpack_ms else "unpack"
     dom_achieved = pack_gbs if dom == "pack" else unpack_gbs
-    if is64:
-        kname = {"pack": "pack_kernel", "unpack": "unpack_kernel"}[dom]
-    elif dom == "pack":
-        kname = "pack_lane_kernel" if L.utl_get_knob(2) == 1 else "pack_quad_kernel"
+    pack_names = {0: "pack_quad_kernel", 1: "pack_lane_kernel", 2: "pack_pair_kernel"}
+    if dom == "pack":
+        kname = ("pack_kernel" if L.utl_get_knob(2) == 0 else "pack_lane_kernel") if is64 else \
+            pack_names.get(L.utl_get_knob(2), "pack_lane_kernel")
+    elif is64:
+        s64 = L.utl_get_knob(8)
+        kname = "unpack_kernel" if s64 == 0 else "unpack_oct64_tma_kernel" if s64 in (1, 2) else "unpack_quad_pipe_kernel"
     else:
-        kname = "unpack_quad_pipe_kernel" if L.utl_get_knob(0) == 1 else "unpack_quad_kernel"
+        s32 = L.utl_get_knob(0)
+        # schedule 8 runs the thread-per-block kernel on batches of small blocks (the exception-heavy one)
+        kname = ("unpack_lane_kernel" if s32 in (8, 9, 10) else "unpack_quad_pipe_kernel" if s32 in (1, 2, 3)
+                 else "unpack_quad_kernel" if s32 == 0 else "unpack_quad_tma_kernel")
     dom_traffic = traffic.get(kname)
     roofline = {"bound": "hbm", "achieved": dom_achieved, "peak": peak, "unit": "GB/s",
                 "frac": dom_achieved / peak, "traffic": (dom_traffic * n) if dom_traffic else None,

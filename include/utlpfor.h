@@ -306,8 +306,7 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *     32 blocks; 2 = persistent warps with the next group's bytes in
  *     flight (cp.async double buffer), staging up to 528 bytes a block;
  *     3 = the same staging up to 264 bytes a block (more warps resident);
- *     1 = 3 or 2 by the batch's mean block length, decided on the device
- *     (the default);
+ *     1 = 3 or 2 by the batch's mean block length, decided on the device;
  *     5 = persistent warps staging each group of 8 blocks with one TMA bulk
  *     copy, three groups in flight, up to 264 bytes a block; 6 = the same
  *     with two groups of up to 528 bytes a block in flight; 4 = 5 or 6 by
@@ -317,8 +316,9 @@ UTL_API int utl_index_stream(const uint8_t *d_packed, size_t packed_len,
  *     trip of the values); 9 = one thread per block (tiles of 32 blocks per
  *     warp, rows written out through a shared-memory chunk), the quad decoder
  *     for blocks it does not take (bitmap exceptions, plain delta, partial,
- *     corrupt or oversized blocks); 8 = 9 for batches of at most 200 bytes a
- *     block on average, else as 1, decided on the device.
+ *     corrupt or oversized blocks); 10 = 9 with the next tile's bytes in
+ *     flight in a second, smaller buffer; 8 = 9 for batches of at most 240
+ *     bytes a block on average, else 2, decided on the device (the default).
  *   UTL_KNOB_PACK_CTAS_PER_SM: cap on resident pack CTAs per SM (0 = the
  *     occupancy maximum).
  *   UTL_KNOB_PACK_SCHEDULE: uint32 pack kernel, 0 = four threads per block

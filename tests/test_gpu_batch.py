@@ -29,7 +29,8 @@ LENS = [1, 128, 300, 0, 257, 1000, 5, 129, 0, 4096, 77]
 
 UNPACK_SCHEDULES = {0: "unpack_tiles", 1: "unpack_pipelined", 2: "unpack_pipelined_wide",
                     3: "unpack_pipelined_narrow", 4: "unpack_tma", 5: "unpack_tma_narrow", 6: "unpack_tma_wide",
-                    7: "unpack_tma_fast", 8: "unpack_thread_auto", 9: "unpack_thread"}
+                    7: "unpack_tma_fast", 8: "unpack_thread_auto", 9: "unpack_thread",
+                    10: "unpack_thread_double"}
 
 
 @pytest.fixture(params=sorted(UNPACK_SCHEDULES), ids=[UNPACK_SCHEDULES[k] for k in sorted(UNPACK_SCHEDULES)])

@@ -892,13 +892,14 @@ __global__ void __launch_bounds__(kQThreads, U64 ? 4 : 5) unpack_quad_pipe_kerne
 // tiles of 32 blocks.  AUTO: launched next to the two pipe instances; each
 // of the three works out from the block offsets whether the batch's mean
 // block length is its class, the other two return at once.
-constexpr int kLUStage = 32 * 264;   // a tile of 32 blocks of up to 264 bytes
-constexpr uint64_t kLaneMean = 200;  // mean packed block length up to which the thread path runs
+constexpr int kLUStage1 = 32 * 264;  // one buffer: a tile of 32 blocks of up to 264 bytes
+constexpr int kLUStage2 = 5120;      // two buffers: tiles of up to 160 bytes a block
+template <int NBUF, int STAGE, int W>
 struct LaneUnpackSmem {
-  uint4 stage[kQWarps][(kLUStage + kQStagePad) / 16];
+  uint4 stage[W][NBUF][(STAGE + kQStagePad) / 16];
   // the output chunk of the tile's 32 blocks; after the chunks, the quads'
   // exception scratch of the fallback (8 x 132 words)
-  uint4 tile[kQWarps][32 * unlane::kTileStride / 16];
+  uint4 tile[W][32 * unlane::kTileStride / 16];
 };
 static_assert(32 * unlane::kTileStride >= 8 * (kBlock + 4) * 4, "fallback scratch");
 
@@ -906,6 +907,7 @@ static_assert(32 * unlane::kTileStride >= 8 * (kBlock + 4) * 4, "fallback scratc
 // the tile's bytes are in stg with block i at ph + (s_i - s_0); otherwise
 // rounds of consecutive blocks that fit are staged here one after the
 // other.  Per-lane inputs are lane i's block values (s, e, first, want, ok).
+template <int STAGE>
 __device__ __forceinline__ void unlane_fallback(const UnpackArgs& a, uint4* stg, uint32_t* scratch, int64_t b0, int nb,
                                              uint32_t todo, bool staged, int ph, uint64_t s, uint64_t e,
                                              uint64_t first, int want, bool ok, int lane) {
@@ -930,7 +932,7 @@ __device__ __forceinline__ void unlane_fallback(const UnpackArgs& a, uint4* stg,
       const uint64_t rs = __shfl_sync(kFull, s, next);
       const int p0 = (int)(((uintptr_t)a.packed + rs) & 15);
       const bool fit = lane >= next && lane < next + 8 && lane < nb && ok && e >= rs &&
-                       (int64_t)(e - rs) + p0 + 16 <= kLUStage;
+                       (int64_t)(e - rs) + p0 + 16 <= STAGE;
       const unsigned fm = __ballot_sync(kFull, fit) >> next;
       const int cnt = max(1, __ffs(~fm) - 1);  // a bad first block is a round of its own
       const bool any = (fm & 1u) != 0;
@@ -983,55 +985,65 @@ __device__ __forceinline__ void unlane_fallback(const UnpackArgs& a, uint4* stg,
   }
 }
 
-template <bool AUTO>
-__global__ void __launch_bounds__(kQThreads, 4) unpack_lane_kernel(UnpackArgs a) {
+// The blocks of tile t as each lane sees its own (lane i: block 32t + i)
+// and whether the tile's bytes fit one staging buffer of STAGE bytes.
+struct LaneTile {
+  uint64_t s, e, first;
+  int want;
+  bool ok, fits;
+};
+__device__ __forceinline__ int lane_tile_nb(const UnpackArgs& a, int64_t t) {
+  return (int)min((int64_t)32, a.n_blocks - t * 32);
+}
+template <int STAGE>
+__device__ __forceinline__ LaneTile lane_tile(const UnpackArgs& a, int64_t t, int lane) {
+  LaneTile q;
+  const int64_t b0 = t * 32;
+  const int nb = lane_tile_nb(a, t);
+  const bool mine = lane < nb;
+  q.s = mine ? a.block_off[b0 + lane] : 0ull;
+  q.e = mine ? a.block_off[b0 + lane + 1] : 0ull;
+  q.ok = mine && q.e >= q.s && q.e - q.s <= (uint64_t)kMaxBlock32 && q.e <= a.packed_len;
+  const uint64_t o0 = __shfl_sync(kFull, q.s, 0), oN = __shfl_sync(kFull, q.e, nb - 1);
+  const int ph = (int)(((uintptr_t)a.packed + o0) & 15);
+  // contiguous and in bounds: every block's end is the next one's start
+  const uint64_t nxt_s = __shfl_down_sync(kFull, q.s, 1);
+  const bool chain = !mine || lane == nb - 1 || nxt_s == q.e;
+  q.fits = __all_sync(kFull, !mine || (q.ok && chain)) && (int64_t)(oN - o0) + ph + 16 <= STAGE;
+  // the values each block decodes to
+  const int s0 = __shfl_sync(kFull, lane == 0 ? stream_of(a.block_start, a.n_streams, b0) : 0, 0);
+  q.first = 0;
+  q.want = 0;
+  if (mine)
+    span_in(a.val_off, a.block_start, stream_from(a.block_start, a.n_streams, s0, b0 + lane), b0 + lane, &q.first,
+            &q.want);
+  return q;
+}
+// Stage tile q's bytes (when they fit) into stg.
+__device__ __forceinline__ void lane_tile_stage(const UnpackArgs& a, const LaneTile& q, int nb, uint4* stg, int lane) {
+  if (q.fits)
+    stage_bytes_async(stg, a.packed, a.packed_len, __shfl_sync(kFull, q.s, 0), __shfl_sync(kFull, q.e, nb - 1), lane);
+}
+
+// Decode tile q (its bytes in stg when q.fits): the thread path's blocks
+// row by row through the chunk tile, then the quad decoder on the rest.
+template <int STAGE>
+__device__ __forceinline__ void lane_tile_decode(const UnpackArgs& a, const LaneTile& q, int64_t b0, int nb,
+                                                 uint4* stg, uint8_t* tileb, int lane) {
   using namespace unlane;
-  extern __shared__ uint4 smem4[];
-  LaneUnpackSmem& S = *(LaneUnpackSmem*)smem4;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (AUTO) {
-    const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
-    if (span > a.lane_mean * (uint64_t)a.n_blocks) return;
-  }
-  const int64_t n_tiles = (a.n_blocks + 31) / 32;
-  const int64_t stride = (int64_t)gridDim.x * kQWarps;
-  uint4* stg = S.stage[warp];
-  uint8_t* tileb = (uint8_t*)S.tile[warp];
-  uint8_t* T = tileb + lane * kTileStride;
   const SmemBytes sb{(const uint32_t*)stg};
-  for (int64_t t = (int64_t)blockIdx.x * kQWarps + warp; t < n_tiles; t += stride) {
-    const int64_t b0 = t * 32;
-    const int nb = (int)min((int64_t)32, a.n_blocks - b0);
-    const bool mine = lane < nb;
-    const uint64_t s = mine ? a.block_off[b0 + lane] : 0ull;
-    const uint64_t e = mine ? a.block_off[b0 + lane + 1] : 0ull;
-    const bool ok = mine && e >= s && e - s <= (uint64_t)kMaxBlock32 && e <= a.packed_len;
-    const uint64_t o0 = __shfl_sync(kFull, s, 0), oN = __shfl_sync(kFull, e, nb - 1);
-    const int ph = (int)(((uintptr_t)a.packed + o0) & 15);
-    // contiguous and in bounds: every block's end is the next one's start
-    const uint64_t nxt_s = __shfl_down_sync(kFull, s, 1);
-    const bool chain = !mine || lane == nb - 1 || nxt_s == e;
-    const bool fits = __all_sync(kFull, !mine || (ok && chain)) && (int64_t)(oN - o0) + ph + 16 <= kLUStage;
-    // the values each block decodes to
-    const int s0 = __shfl_sync(kFull, lane == 0 ? stream_of(a.block_start, a.n_streams, b0) : 0, 0);
-    uint64_t first = 0;
-    int want = 0;
-    if (mine) span_in(a.val_off, a.block_start, stream_from(a.block_start, a.n_streams, s0, b0 + lane), b0 + lane,
-                      &first, &want);
-    if (fits) {
-      stage_bytes_async(stg, a.packed, a.packed_len, o0, oN, lane);
-      cp_async_commit();
-      asm volatile("cp.async.wait_all;" ::: "memory");
-    }
-    __syncwarp();
-    Plan f;
-    const bool fast = fits && mine && plan(sb, ph + (int)(s - o0), (int)(e - s), want, f);
-    const uint32_t fastm = __ballot_sync(kFull, fast);
-    if (fastm) {
-      uint32_t cur[16], nxt[16], acc[16];
+  uint8_t* T = tileb + lane * kTileStride;
+  const bool mine = lane < nb;
+  const uint64_t o0 = __shfl_sync(kFull, q.s, 0);
+  const int ph = (int)(((uintptr_t)a.packed + o0) & 15);
+  Plan f;
+  const bool fast = q.fits && mine && plan(sb, ph + (int)(q.s - o0), (int)(q.e - q.s), q.want, f);
+  const uint32_t fastm = __ballot_sync(kFull, fast);
+  if (fastm) {
+      uint32_t cur[16], nxt[16];
       int wi = 0, ex = 0, np = 256, doff = 0;
 #pragma unroll
-      for (int i = 0; i < 16; i++) cur[i] = nxt[i] = acc[i] = 0;
+      for (int i = 0; i < 16; i++) cur[i] = nxt[i] = 0;
       if (fast) {
         if (f.bw > 0) load_words(sb, f.pay, cur);
         if (f.bw > 4) load_words(sb, f.pay + 64, nxt);
@@ -1049,11 +1061,17 @@ __global__ void __launch_bounds__(kQThreads, 4) unpack_lane_kernel(UnpackArgs a)
 #pragma unroll
             for (int i = 0; i < 16; i++) y[i] = __funnelshift_r(cur[i], nxt[i], sh) & f.mask;
             if (f.delta) {
-              // zigzag delta (delta.go:50-115): the per-lane running sum
+              // zigzag delta (delta.go:50-115): the per-lane running sum;
+              // the previous row is still in the chunk tile's other slot
+              // (the chunk copy-out only reads it), with the FOR base added
+              const uint8_t* pr = T + 64 * ((r + kRows - 1) % kRows);
 #pragma unroll
-              for (int i = 0; i < 16; i++) {
-                acc[i] = (v == 0 ? 0u : acc[i]) + zz_dec(y[i]);
-                y[i] = acc[i];
+              for (int i = 0; i < 4; i++) {
+                const uint4 p4 = *(const uint4*)(pr + 16 * i);
+                const uint32_t pv[4] = {p4.x, p4.y, p4.z, p4.w};
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                  y[4 * i + k] = (v == 0 ? 0u : pv[k] - f.base) + zz_dec(y[4 * i + k]);
               }
             }
 #pragma unroll
@@ -1087,11 +1105,13 @@ __global__ void __launch_bounds__(kQThreads, 4) unpack_lane_kernel(UnpackArgs a)
 #pragma unroll 1
         for (int it = 0; it < 32 / kBlocksPerStore; it++) {
           const int i = it * kBlocksPerStore + lane / kLanesPerBlock;
-          const uint64_t fi = __shfl_sync(kFull, first, i);
+          const uint64_t fi = __shfl_sync(kFull, q.first, i);
           if ((fastm >> i) & 1u) {
             const uint4 val = *(const uint4*)(tileb + i * kTileStride + 16 * part);
             uint32_t* op = (uint32_t*)a.values + fi + 16 * kRows * c + 4 * part;
-            if ((fi & 3) == 0) {
+            // 16-byte stores only at 16-byte addresses (the host pipeline's
+            // pieces start their values at any value index)
+            if (((uintptr_t)op & 15) == 0) {
               __stcs((uint4*)op, val);
             } else {
               op[0] = val.x;
@@ -1103,13 +1123,61 @@ __global__ void __launch_bounds__(kQThreads, 4) unpack_lane_kernel(UnpackArgs a)
         }
         __syncwarp();
       }
-      if (fast && a.block_status) a.block_status[b0 + lane] = kOK;
-    }
-    const uint32_t todo = __ballot_sync(kFull, mine && !fast);
-    if (todo)
-      unlane_fallback(a, stg, (uint32_t*)tileb, b0, nb, todo, fits, ph, s, e, first, want, ok, lane);
-    __syncwarp();
+    if (fast && a.block_status) a.block_status[b0 + lane] = kOK;
   }
+  const uint32_t todo = __ballot_sync(kFull, mine && !fast);
+  if (todo)
+    unlane_fallback<STAGE>(a, stg, (uint32_t*)tileb, b0, nb, todo, q.fits, ph, q.s, q.e, q.first, q.want, q.ok, lane);
+}
+
+// NBUF 1: each tile is staged and waited for at the top of its turn; NBUF
+// 2: the next tile's bytes are in flight while this one decodes (smaller
+// buffers, tiles of up to 160 bytes a block; larger tiles take the quad
+// decoder with their own staging).  W warps per CTA.
+template <bool AUTO, int NBUF, int STAGE, int W>
+__global__ void __launch_bounds__(32 * W, 16 / W) unpack_lane_kernel(UnpackArgs a) {
+  extern __shared__ uint4 smem4[];
+  LaneUnpackSmem<NBUF, STAGE, W>& S = *(LaneUnpackSmem<NBUF, STAGE, W>*)smem4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (AUTO) {
+    const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
+    if (span > a.lane_mean * (uint64_t)a.n_blocks) return;
+  }
+  const int64_t n_tiles = (a.n_blocks + 31) / 32;
+  const int64_t stride = (int64_t)gridDim.x * W;
+  uint8_t* tileb = (uint8_t*)S.tile[warp];
+  int64_t t = (int64_t)blockIdx.x * W + warp;
+  if (t >= n_tiles) return;
+  LaneTile cur = lane_tile<STAGE>(a, t, lane);
+  if (NBUF == 2) {
+    lane_tile_stage(a, cur, lane_tile_nb(a, t), S.stage[warp][0], lane);
+    cp_async_commit();
+  }
+  for (int it = 0; t < n_tiles; it++, t += stride) {
+    const int buf = NBUF == 2 ? (it & 1) : 0;
+    LaneTile nxt;
+    if constexpr (NBUF == 2) {
+      if (t + stride < n_tiles) {
+        nxt = lane_tile<STAGE>(a, t + stride, lane);
+        lane_tile_stage(a, nxt, lane_tile_nb(a, t + stride), S.stage[warp][buf ^ 1], lane);
+      }
+      cp_async_commit();
+      cp_async_wait1();
+    } else {
+      lane_tile_stage(a, cur, lane_tile_nb(a, t), S.stage[warp][0], lane);
+      cp_async_commit();
+      asm volatile("cp.async.wait_all;" ::: "memory");
+    }
+    __syncwarp();
+    lane_tile_decode<STAGE>(a, cur, t * 32, lane_tile_nb(a, t), S.stage[warp][buf], tileb, lane);
+    __syncwarp();
+    if constexpr (NBUF == 2) {
+      cur = nxt;
+    } else {
+      if (t + stride < n_tiles) cur = lane_tile<STAGE>(a, t + stride, lane);
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // TMA-staged pipelined unpack (utl_unpack.cuh): persistent warps over
@@ -2724,7 +2792,7 @@ struct DevCfg {
   int tma_ctas = 0;              // unpack_quad_tma_kernel, narrow staging (3 stages)
   int tma_wide_ctas = 0;         // unpack_quad_tma_kernel, wide staging (2 stages)
   int oct64_ctas[2] = {0, 0};    // unpack_oct64_tma_kernel, 2 / 3 stages
-  int lane_unpack_ctas = 0;       // unpack_lane_kernel
+  int lane_unpack_ctas[2] = {0, 0};  // unpack_lane_kernel, one / two staging buffers
   int pipe64_ctas[3] = {0, 0, 0};  // unpack_quad_pipe_kernel for uint64: narrow, wide, wide single buffer
   int pack_ctas[2] = {0, 0};     // pack_kernel<false/true>
   // Mapped pinned pair the uint32 lane pack's last block fills with the
@@ -2847,13 +2915,13 @@ static cudaError_t unpack_pipe(const UnpackArgs& a, cudaStream_t st, int ctas) {
   note_launch(1);
   return cudaGetLastError();
 }
-template <bool AUTO>
+template <bool AUTO, int NBUF, int STAGE, int W>
 static cudaError_t unpack_lane(const UnpackArgs& a, cudaStream_t st, int ctas) {
   const int64_t tiles = (a.n_blocks + 31) / 32;
   int64_t grid = (int64_t)num_sms() * unpack_ctas(ctas);
-  const int64_t need = (tiles + kQWarps - 1) / kQWarps;
+  const int64_t need = (tiles + W - 1) / W;
   if (grid > need) grid = need;
-  unpack_lane_kernel<AUTO><<<(unsigned)grid, kQThreads, sizeof(LaneUnpackSmem), st>>>(a);
+  unpack_lane_kernel<AUTO, NBUF, STAGE, W><<<(unsigned)grid, 32 * W, sizeof(LaneUnpackSmem<NBUF, STAGE, W>), st>>>(a);
   note_launch(1);
   return cudaGetLastError();
 }
@@ -2869,7 +2937,7 @@ static cudaError_t unpack_tma(const UnpackArgs& a, cudaStream_t st, int ctas) {
   return cudaGetLastError();
 }
 // UTL_KNOB_UNPACK_SCHEDULE (include/utlpfor.h)
-static int g_unpack_schedule = 1;
+static int g_unpack_schedule = 8;
 static int g_pack_cap = 0;
 static int g_pack_schedule = 1;
 // Test knobs: the polls of every bounded wait (0 = the default 2^22), and
@@ -2945,9 +3013,13 @@ static cudaError_t setup_device(int dev, DevCfg& c) {
   if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, false, true>, qw)) != cudaSuccess) return e;
   c.pipe64_ctas[0] = occupancy(unpack_quad_pipe_kernel<kPStageWide, false, true>, kQThreads, qn);
   c.pipe64_ctas[1] = occupancy(unpack_quad_pipe_kernel<kP64StageWide, false, true>, kQThreads, qw);
-  if ((e = set_smem(unpack_lane_kernel<true>, sizeof(LaneUnpackSmem))) != cudaSuccess) return e;
-  if ((e = set_smem(unpack_lane_kernel<false>, sizeof(LaneUnpackSmem))) != cudaSuccess) return e;
-  c.lane_unpack_ctas = occupancy(unpack_lane_kernel<false>, kQThreads, sizeof(LaneUnpackSmem));
+  const size_t lu1 = sizeof(LaneUnpackSmem<1, kLUStage1, 4>), lu2 = sizeof(LaneUnpackSmem<2, kLUStage2, 2>);
+  if ((e = set_smem(unpack_lane_kernel<true, 1, kLUStage1, 4>, lu1)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_lane_kernel<false, 1, kLUStage1, 4>, lu1)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_lane_kernel<true, 2, kLUStage2, 2>, lu2)) != cudaSuccess) return e;
+  if ((e = set_smem(unpack_lane_kernel<false, 2, kLUStage2, 2>, lu2)) != cudaSuccess) return e;
+  c.lane_unpack_ctas[0] = occupancy(unpack_lane_kernel<false, 1, kLUStage1, 4>, 128, lu1);
+  c.lane_unpack_ctas[1] = occupancy(unpack_lane_kernel<false, 2, kLUStage2, 2>, 64, lu2);
   const size_t q1 = sizeof(QuadPipeSmem<kP64StageWide, 1>);
   if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, true, true, 1>, q1)) != cudaSuccess) return e;
   if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, false, true, 1>, q1)) != cudaSuccess) return e;
@@ -3046,16 +3118,15 @@ cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
   cudaError_t e = dev_cfg(&c);
   if (e != cudaSuccess) return e;
   if (!u64) {
-    if (g_unpack_schedule == 8) {  // thread per block for small blocks, else as 1; decided on the device
+    if (g_unpack_schedule == 8) {  // thread per block or the wide pipeline by the mean block length, on the device
       UnpackArgs b = a;
-      b.lane_mean = kLaneMean;
-      e = unpack_lane<true>(b, st, c->lane_unpack_ctas);
-      if (e != cudaSuccess) return e;
-      e = unpack_pipe<kPStageNarrow, true>(b, st, c->pipe_ctas);
+      b.lane_mean = kWideMean;
+      e = unpack_lane<true, 1, kLUStage1, 4>(b, st, c->lane_unpack_ctas[0]);
       if (e != cudaSuccess) return e;
       return unpack_pipe<kPStageWide, true>(b, st, c->pipe_wide_ctas);
     }
-    if (g_unpack_schedule == 9) return unpack_lane<false>(a, st, c->lane_unpack_ctas);
+    if (g_unpack_schedule == 9) return unpack_lane<false, 1, kLUStage1, 4>(a, st, c->lane_unpack_ctas[0]);
+    if (g_unpack_schedule == 10) return unpack_lane<false, 2, kLUStage2, 2>(a, st, c->lane_unpack_ctas[1]);
     if (g_unpack_schedule == 1) {  // by the batch's mean block length, decided on the device
       e = unpack_pipe<kPStageNarrow, true>(a, st, c->pipe_ctas);
       if (e != cudaSuccess) return e;
@@ -3141,7 +3212,7 @@ cudaError_t plain_get(bool u64, int pos, const uint8_t* src, int64_t staged, int
 int set_knob(int knob, int value) {
   switch (knob) {
     case 0:  // UTL_KNOB_UNPACK_SCHEDULE
-      if (value < 0 || value > 9) return -1;
+      if (value < 0 || value > 10) return -1;
       g_unpack_schedule = value;
       return 0;
     case 1:  // UTL_KNOB_PACK_CTAS_PER_SM (0 = occupancy maximum)

@@ -13,7 +13,9 @@ that file (if any) for the current GPU and sets the knobs.  Knobs
   0 UTL_KNOB_UNPACK_SCHEDULE     0 tiles; 1-3 cp.async double buffer (auto,
                                  wide, narrow staging); 4-6 TMA bulk staging
                                  (auto, three narrow groups, two wide groups
-                                 in flight per warp)
+                                 in flight per warp); 8 a thread per block
+                                 for small blocks, else the wide cp.async
+                                 pipeline
   7 UTL_KNOB_UNPACK_CTAS_PER_SM  warps per SM of the unpack (4 per CTA):
                                  0 occupancy maximum, else a cap
 The pack schedule (with the window left to its per-batch choice) is swept
@@ -32,12 +34,12 @@ from ._lib import load
 HERE = os.path.dirname(os.path.abspath(__file__))
 TUNED = os.path.join(HERE, "tuned")
 # Candidates are the settings that suit any batch: the window and the
-# unpack staging size stay chosen per batch (window 0, unpack schedules 1
-# and 4 pick by block density), so a setting tuned on one workload cannot
+# unpack staging size stay chosen per batch (window 0, unpack schedules 1,
+# 4 and 8 pick by block density), so a setting tuned on one workload cannot
 # slow down a batch of much larger blocks.
 PACK_SHAPES = [(1, 0), (2, 0), (0, 0)]  # (schedule, window)
 PACK_CAPS = [0, 16, 12, 8]
-UNPACK_SCHEDULES = [1, 4, 0]
+UNPACK_SCHEDULES = [8, 1, 4, 0]
 UNPACK_CAPS = [0, 4, 3, 2]
 KNOBS = ("0", "1", "2", "6", "7")
 
