@@ -658,9 +658,10 @@ def main():
         kname = "unpack_kernel" if s64 == 0 else "unpack_oct64_tma_kernel" if s64 in (1, 2) else "unpack_quad_pipe_kernel"
     else:
         s32 = L.utl_get_knob(0)
-        # schedule 8 runs the thread-per-block kernel on batches of small blocks (the exception-heavy one)
-        kname = ("unpack_lane_kernel" if s32 in (8, 9, 10) else "unpack_quad_pipe_kernel" if s32 in (1, 2, 3)
-                 else "unpack_quad_kernel" if s32 == 0 else "unpack_quad_tma_kernel")
+        # schedule 8: one kernel, the thread-per-block path on batches of small blocks (the exception-heavy one)
+        kname = ("unpack_auto_kernel" if s32 == 8 else "unpack_lane_kernel" if s32 in (9, 10)
+                 else "unpack_quad_pipe_kernel" if s32 in (1, 2, 3) else "unpack_quad_kernel" if s32 == 0
+                 else "unpack_quad_tma_kernel")
     dom_traffic = traffic.get(kname)
     roofline = {"bound": "hbm", "achieved": dom_achieved, "peak": peak, "unit": "GB/s",
                 "frac": dom_achieved / peak, "traffic": (dom_traffic * n) if dom_traffic else None,

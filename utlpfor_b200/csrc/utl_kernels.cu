@@ -763,18 +763,11 @@ __device__ __forceinline__ void quad64_block(const SmemBytes& sb, int blk, int l
 // NBUF 1: one staging buffer per warp, filled and waited for at the top of
 // each group (twice the resident warps of the double buffer for the large
 // uint64 budget, which hides the wait instead).
-template <int STAGE, bool AUTO, bool U64 = false, int NBUF = 2>
-__global__ void __launch_bounds__(kQThreads, U64 ? 4 : 5) unpack_quad_pipe_kernel(UnpackArgs a) {
-  extern __shared__ uint4 smem4[];
+template <int STAGE, bool U64, int NBUF>
+__device__ __forceinline__ void pipe_body(const UnpackArgs& a, uint4* smem4) {
   QuadPipeSmem<STAGE, NBUF>& S = *(QuadPipeSmem<STAGE, NBUF>*)smem4;
   constexpr int kMaxB = U64 ? kMaxBlock64 : kMaxBlock32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (AUTO) {
-    const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
-    const bool wide = span > (U64 ? kWideMean64 : kWideMean) * (uint64_t)a.n_blocks;
-    if (wide != (STAGE == (U64 ? kP64StageWide : kPStageWide))) return;
-    if (!wide && span <= a.lane_mean * (uint64_t)a.n_blocks) return;
-  }
   const int q = lane >> 2, j = lane & 3;
   const unsigned qm = quad::quad_mask(lane);
   const int64_t n_groups = (a.n_blocks + 7) / 8;
@@ -886,6 +879,18 @@ __global__ void __launch_bounds__(kQThreads, U64 ? 4 : 5) unpack_quad_pipe_kerne
     }
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+template <int STAGE, bool AUTO, bool U64 = false, int NBUF = 2>
+__global__ void __launch_bounds__(kQThreads, U64 ? 4 : 5) unpack_quad_pipe_kernel(UnpackArgs a) {
+  extern __shared__ uint4 smem4[];
+  if (AUTO) {
+    const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
+    const bool wide = span > (U64 ? kWideMean64 : kWideMean) * (uint64_t)a.n_blocks;
+    if (wide != (STAGE == (U64 ? kP64StageWide : kPStageWide))) return;
+    if (!wide && span <= a.lane_mean * (uint64_t)a.n_blocks) return;
+  }
+  pipe_body<STAGE, U64, NBUF>(a, smem4);
 }
 
 // Thread-per-block uint32 unpack (utl_unlane.cuh): persistent warps over
@@ -1053,7 +1058,7 @@ __device__ __forceinline__ void lane_tile_decode(const UnpackArgs& a, const Lane
 #pragma unroll 1
       for (int c = 0; c < 8 / kRows; c++) {
         if (fast) {
-#pragma unroll 1
+#pragma unroll
           for (int r = 0; r < kRows; r++) {
             const int v = c * kRows + r;
             const int sh = v * f.bw - 32 * wi;
@@ -1134,15 +1139,10 @@ __device__ __forceinline__ void lane_tile_decode(const UnpackArgs& a, const Lane
 // 2: the next tile's bytes are in flight while this one decodes (smaller
 // buffers, tiles of up to 160 bytes a block; larger tiles take the quad
 // decoder with their own staging).  W warps per CTA.
-template <bool AUTO, int NBUF, int STAGE, int W>
-__global__ void __launch_bounds__(32 * W, 16 / W) unpack_lane_kernel(UnpackArgs a) {
-  extern __shared__ uint4 smem4[];
+template <int NBUF, int STAGE, int W>
+__device__ __forceinline__ void lane_body(const UnpackArgs& a, uint4* smem4) {
   LaneUnpackSmem<NBUF, STAGE, W>& S = *(LaneUnpackSmem<NBUF, STAGE, W>*)smem4;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (AUTO) {
-    const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
-    if (span > a.lane_mean * (uint64_t)a.n_blocks) return;
-  }
   const int64_t n_tiles = (a.n_blocks + 31) / 32;
   const int64_t stride = (int64_t)gridDim.x * W;
   uint8_t* tileb = (uint8_t*)S.tile[warp];
@@ -1178,6 +1178,31 @@ __global__ void __launch_bounds__(32 * W, 16 / W) unpack_lane_kernel(UnpackArgs 
     }
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+template <bool AUTO, int NBUF, int STAGE, int W>
+__global__ void __launch_bounds__(32 * W, 16 / W) unpack_lane_kernel(UnpackArgs a) {
+  extern __shared__ uint4 smem4[];
+  if (AUTO) {
+    const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
+    if (span > a.lane_mean * (uint64_t)a.n_blocks) return;
+  }
+  lane_body<NBUF, STAGE, W>(a, smem4);
+}
+
+// The default uint32 unpack in one launch: the thread-per-block path for
+// batches of at most kWideMean bytes a block on average, the quad pipeline
+// with the large staging otherwise (both persistent, 4 warps per CTA, at
+// most as much shared memory as the launch provides), chosen from the
+// block offsets by every CTA alike.
+constexpr size_t kAutoSmem = sizeof(LaneUnpackSmem<1, kLUStage1, 4>) > sizeof(QuadPipeSmem<kPStageWide, 2>)
+                                 ? sizeof(LaneUnpackSmem<1, kLUStage1, 4>)
+                                 : sizeof(QuadPipeSmem<kPStageWide, 2>);
+__global__ void __launch_bounds__(kQThreads, 4) unpack_auto_kernel(UnpackArgs a) {
+  extern __shared__ uint4 smem4[];
+  const uint64_t span = a.block_off[a.n_blocks] - a.block_off[0];
+  if (span <= kWideMean * (uint64_t)a.n_blocks) lane_body<1, kLUStage1, 4>(a, smem4);
+  else pipe_body<kPStageWide, false, 2>(a, smem4);
 }
 
 // TMA-staged pipelined unpack (utl_unpack.cuh): persistent warps over
@@ -2793,6 +2818,7 @@ struct DevCfg {
   int tma_wide_ctas = 0;         // unpack_quad_tma_kernel, wide staging (2 stages)
   int oct64_ctas[2] = {0, 0};    // unpack_oct64_tma_kernel, 2 / 3 stages
   int lane_unpack_ctas[2] = {0, 0};  // unpack_lane_kernel, one / two staging buffers
+  int auto_unpack_ctas = 0;          // unpack_auto_kernel
   int pipe64_ctas[3] = {0, 0, 0};  // unpack_quad_pipe_kernel for uint64: narrow, wide, wide single buffer
   int pack_ctas[2] = {0, 0};     // pack_kernel<false/true>
   // Mapped pinned pair the uint32 lane pack's last block fills with the
@@ -2915,6 +2941,16 @@ static cudaError_t unpack_pipe(const UnpackArgs& a, cudaStream_t st, int ctas) {
   note_launch(1);
   return cudaGetLastError();
 }
+static cudaError_t unpack_auto(const UnpackArgs& a, cudaStream_t st, int ctas) {
+  // persistent over the finer of the two paths' work items (8-block groups)
+  const int64_t groups = (a.n_blocks + 7) / 8;
+  int64_t grid = (int64_t)num_sms() * unpack_ctas(ctas);
+  const int64_t need = (groups + kQWarps - 1) / kQWarps;
+  if (grid > need) grid = need;
+  unpack_auto_kernel<<<(unsigned)grid, kQThreads, kAutoSmem, st>>>(a);
+  note_launch(1);
+  return cudaGetLastError();
+}
 template <bool AUTO, int NBUF, int STAGE, int W>
 static cudaError_t unpack_lane(const UnpackArgs& a, cudaStream_t st, int ctas) {
   const int64_t tiles = (a.n_blocks + 31) / 32;
@@ -3020,6 +3056,8 @@ static cudaError_t setup_device(int dev, DevCfg& c) {
   if ((e = set_smem(unpack_lane_kernel<false, 2, kLUStage2, 2>, lu2)) != cudaSuccess) return e;
   c.lane_unpack_ctas[0] = occupancy(unpack_lane_kernel<false, 1, kLUStage1, 4>, 128, lu1);
   c.lane_unpack_ctas[1] = occupancy(unpack_lane_kernel<false, 2, kLUStage2, 2>, 64, lu2);
+  if ((e = set_smem(unpack_auto_kernel, kAutoSmem)) != cudaSuccess) return e;
+  c.auto_unpack_ctas = occupancy(unpack_auto_kernel, kQThreads, kAutoSmem);
   const size_t q1 = sizeof(QuadPipeSmem<kP64StageWide, 1>);
   if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, true, true, 1>, q1)) != cudaSuccess) return e;
   if ((e = set_smem(unpack_quad_pipe_kernel<kP64StageWide, false, true, 1>, q1)) != cudaSuccess) return e;
@@ -3118,13 +3156,8 @@ cudaError_t unpack(bool u64, const UnpackArgs& a, cudaStream_t st) {
   cudaError_t e = dev_cfg(&c);
   if (e != cudaSuccess) return e;
   if (!u64) {
-    if (g_unpack_schedule == 8) {  // thread per block or the wide pipeline by the mean block length, on the device
-      UnpackArgs b = a;
-      b.lane_mean = kWideMean;
-      e = unpack_lane<true, 1, kLUStage1, 4>(b, st, c->lane_unpack_ctas[0]);
-      if (e != cudaSuccess) return e;
-      return unpack_pipe<kPStageWide, true>(b, st, c->pipe_wide_ctas);
-    }
+    // thread per block or the wide pipeline by the mean block length, on the device, in one launch
+    if (g_unpack_schedule == 8) return unpack_auto(a, st, c->auto_unpack_ctas);
     if (g_unpack_schedule == 9) return unpack_lane<false, 1, kLUStage1, 4>(a, st, c->lane_unpack_ctas[0]);
     if (g_unpack_schedule == 10) return unpack_lane<false, 2, kLUStage2, 2>(a, st, c->lane_unpack_ctas[1]);
     if (g_unpack_schedule == 1) {  // by the batch's mean block length, decided on the device
