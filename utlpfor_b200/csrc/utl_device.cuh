@@ -703,6 +703,47 @@ __device__ __forceinline__ int bitmap_rank128(const GlobalBytes& g, int64_t bm, 
   return __popcll(w0) + __popcll(w1 & ((1ull << (8 * (byte_idx - 8) + bit_idx)) - 1ull));
 }
 
+// Whether a block's exceptions apply as the full unpack applies them when
+// each is looked up by its own position: a position list strictly
+// increasing below the count, or a bitmap (bits past the count dropped)
+// with no more bits than exceptions.  x: the exception index, xlen bytes
+// from there to the block's end.
+__device__ __forceinline__ bool exc_in_order(const GlobalBytes& g, int64_t x, int64_t xlen, int exc, int count) {
+  if (exc <= 16) {
+    if (xlen < exc) return false;
+    int prev = -1;
+    for (int i = 0; i < exc; i++) {
+      const int p = (int)g.u8(x + i);
+      if (p <= prev || p >= count) return false;
+      prev = p;
+    }
+    return true;
+  }
+  if (xlen < 16) return false;
+  int pop = 0;
+  for (int k = 0; k < 4; k++) {
+    uint32_t m = g.u32(x + 4 * k);
+    const int lo = 32 * k;
+    if (count <= lo) m = 0;
+    else if (count < lo + 32) m &= (1u << (count - lo)) - 1u;
+    pop += __popc(m);
+  }
+  return pop <= exc;
+}
+
+// exceptions.go:63-80: the StreamVByte control bytes (at x, len bytes of
+// control and data) and the data they size fit.
+__device__ __forceinline__ bool svb_controls_fit(const GlobalBytes& g, int64_t x, int64_t len, int exc) {
+  const int nc = (exc + 3) >> 2;
+  int64_t total = 0;
+  for (int c = 0; c < nc; c++) {
+    const uint32_t b = g.u8(x + c);
+    const int slots = min(4, exc - 4 * c);
+    for (int s2 = 0; s2 < slots; s2++) total += (int64_t)((b >> (2 * s2)) & 3) + 1;
+  }
+  return nc + total <= len;
+}
+
 // Result of a thread-level Get on one (sub-)block.  need_full asks the warp
 // to resolve the value with a full block unpack (get.go:174-181).
 struct GetResult {
@@ -780,9 +821,22 @@ __device__ GetResult thread_get_u32(const GlobalBytes& g, int64_t len, int pos, 
   }
   const int pil = pos >> 4;
   if (pil > delta_full_unpack_threshold(bw)) {
-    r.need_full = true;
-    r.end = end;
-    return r;
+    // The reference unpacks the whole block here (get.go:174-181), for speed
+    // only.  For a zigzag delta block (no overflow is possible) whose
+    // exceptions are in order, the lane walk below gives the value the full
+    // unpack gives, and of the full unpack's checks only the StreamVByte
+    // control validation (exceptions.go:63-80) is not already done above.
+    // Other blocks -- plain delta, whose overflow anywhere in the block the
+    // full unpack reports, or exceptions out of order -- go to the warp.
+    if (!zz || (has_exc && !exc_in_order(gb, xs, end - xs, exc, count))) {
+      r.need_full = true;
+      r.end = end;
+      return r;
+    }
+    if (has_exc && !svb_controls_fit(gb, xs + isz, end - xs - isz, exc)) {
+      r.status = kErrInvalidBuffer;
+      return r;
+    }
   }
   // getValueWithDelta, get.go:250-285
   const int lane = pos & 15;
