@@ -1044,6 +1044,9 @@ __device__ __forceinline__ void lane_tile_decode(const UnpackArgs& a, const Lane
   Plan f;
   const bool fast = q.fits && mine && plan(sb, ph + (int)(q.s - o0), (int)(q.e - q.s), q.want, f);
   const uint32_t fastm = __ballot_sync(kFull, fast);
+  // the block's first value index, in the padding after its chunk rows: the
+  // copy-out reads it with one shared load instead of two shuffles
+  *(uint64_t*)(T + 64 * kRows) = q.first;
   if (fastm) {
       uint32_t cur[16], nxt[16];
       int wi = 0, ex = 0, np = 256, doff = 0;
@@ -1107,10 +1110,10 @@ __device__ __forceinline__ void lane_tile_decode(const UnpackArgs& a, const Lane
         __syncwarp();
         // the chunk's rows of every thread-path block, 16 bytes per lane
         const int part = lane % kLanesPerBlock;
-#pragma unroll 1
+#pragma unroll 4
         for (int it = 0; it < 32 / kBlocksPerStore; it++) {
           const int i = it * kBlocksPerStore + lane / kLanesPerBlock;
-          const uint64_t fi = __shfl_sync(kFull, q.first, i);
+          const uint64_t fi = *(const uint64_t*)(tileb + i * kTileStride + 64 * kRows);
           if ((fastm >> i) & 1u) {
             const uint4 val = *(const uint4*)(tileb + i * kTileStride + 16 * part);
             uint32_t* op = (uint32_t*)a.values + fi + 16 * kRows * c + 4 * part;

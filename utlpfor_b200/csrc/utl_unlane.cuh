@@ -29,7 +29,8 @@ namespace utl {
 namespace unlane {
 
 constexpr int kRows = 2;                        // rows of every block per output chunk
-constexpr int kTileStride = 64 * kRows + 16;    // bytes per block in the chunk tile (+16: conflict-free stores)
+constexpr int kTileStride = 64 * kRows + 16;    // bytes per block in the chunk tile (+16: conflict-free stores;
+                                                // its first 8 bytes hold the block's first value index)
 constexpr int kLanesPerBlock = 64 * kRows / 16;  // lanes that write one block's chunk
 constexpr int kBlocksPerStore = 32 / kLanesPerBlock;
 
