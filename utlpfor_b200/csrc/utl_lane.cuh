@@ -368,11 +368,40 @@ __device__ __forceinline__ void pack_group<16>(const uint32_t (&w)[8][4], uint32
   for (int i = 0; i < 4; i++) put_seg(pw, d4, sh, i, g, x[i]);
 }
 
+// The same at any width (multiple of 4, at most 32) with runtime shifts:
+// a word of the four lanes is complete when a row reaches its end, and the
+// part of that row's value above it starts the next word.  Eight copies of
+// the segment store instead of the 36 of the per-width code.
+__device__ __forceinline__ void pack_group_any(const uint32_t (&w)[8][4], int bw, uint32_t* pw, int d4, int sh,
+                                               int g) {
+  if (bw == 0) return;
+  const uint32_t mask = bw >= 32 ? 0xFFFFFFFFu : ((1u << bw) - 1u);
+  uint32_t acc[4] = {0, 0, 0, 0};
+  int pos = 0, wi = 0;
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    uint32_t m[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      m[k] = w[r][k] & mask;
+      acc[k] |= m[k] << pos;
+    }
+    pos += bw;
+    if (pos >= 32) {
+      put_seg(pw, d4, sh, wi, g, acc);
+      wi++;
+      pos -= 32;
+#pragma unroll
+      for (int k = 0; k < 4; k++) acc[k] = pos ? (m[k] >> (bw - pos)) : 0u;
+    }
+  }
+}
+
 // Write the block at o (shared memory): header, StreamVByte length, FOR
 // base, the UTL payload (scalar.go:7-59: lane L's eight values packed LSB
 // first into bw/4 words, word w of lane L at byte 64w + 4L), then the
 // exception index and StreamVByte data (exceptions.go:138-186).
-template <bool DELTA, bool EXC>
+template <bool DELTA, bool EXC, bool ANY_WIDTH = false>
 __device__ void write_block(const Plan& p, const uint4* s4, uint8_t* o) {
   put_bytes(o, p.header, 4);
   int m = 4;
@@ -412,16 +441,20 @@ __device__ void write_block(const Plan& p, const uint4* s4, uint8_t* o) {
 #pragma unroll
       for (int q = 0; q < 4; q++) bm[q] |= f[q] << (4 * g);
     }
-    switch (bw) {
-      case 4: pack_group<4>(w, pw, d4, sh, g); break;
-      case 8: pack_group<8>(w, pw, d4, sh, g); break;
-      case 12: pack_group<12>(w, pw, d4, sh, g); break;
-      case 16: pack_group<16>(w, pw, d4, sh, g); break;
-      case 20: pack_group<20>(w, pw, d4, sh, g); break;
-      case 24: pack_group<24>(w, pw, d4, sh, g); break;
-      case 28: pack_group<28>(w, pw, d4, sh, g); break;
-      case 32: pack_group<32>(w, pw, d4, sh, g); break;
-      default: break;  // bw 0: no payload
+    if constexpr (ANY_WIDTH) {
+      pack_group_any(w, bw, pw, d4, sh, g);
+    } else {
+      switch (bw) {
+        case 4: pack_group<4>(w, pw, d4, sh, g); break;
+        case 8: pack_group<8>(w, pw, d4, sh, g); break;
+        case 12: pack_group<12>(w, pw, d4, sh, g); break;
+        case 16: pack_group<16>(w, pw, d4, sh, g); break;
+        case 20: pack_group<20>(w, pw, d4, sh, g); break;
+        case 24: pack_group<24>(w, pw, d4, sh, g); break;
+        case 28: pack_group<28>(w, pw, d4, sh, g); break;
+        case 32: pack_group<32>(w, pw, d4, sh, g); break;
+        default: break;  // bw 0: no payload
+      }
     }
   }
   if (EXC && p.exc) {
