@@ -662,7 +662,7 @@ def main():
         kname = ("unpack_auto_kernel" if s32 == 8 else "unpack_lane_kernel" if s32 in (9, 10)
                  else "unpack_quad_pipe_kernel" if s32 in (1, 2, 3) else "unpack_quad_kernel" if s32 == 0
                  else "unpack_quad_tma_kernel")
-    dom_traffic = traffic.get(kname)
+    dom_traffic = traffic.get(kname + ("_u64" if is64 else ""))  # per-value DRAM bytes of that kernel on that width
     roofline = {"bound": "hbm", "achieved": dom_achieved, "peak": peak, "unit": "GB/s",
                 "frac": dom_achieved / peak, "traffic": (dom_traffic * n) if dom_traffic else None,
                 "kernel": kname, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
