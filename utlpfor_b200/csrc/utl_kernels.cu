@@ -1069,7 +1069,7 @@ __device__ __forceinline__ void lane_tile_decode(const UnpackArgs& a, const Lane
 #pragma unroll
             for (int i = 0; i < 16; i++) y[i] = __funnelshift_r(cur[i], nxt[i], sh) & f.mask;
             if (f.delta) {
-              // zigzag delta (delta.go:50-115): the per-lane running sum;
+              // delta (delta.go:50-115): the per-lane running sum;
               // the previous row is still in the chunk tile's other slot
               // (the chunk copy-out only reads it), with the FOR base added
               const uint8_t* pr = T + 64 * ((r + kRows - 1) % kRows);
@@ -1079,7 +1079,7 @@ __device__ __forceinline__ void lane_tile_decode(const UnpackArgs& a, const Lane
                 const uint32_t pv[4] = {p4.x, p4.y, p4.z, p4.w};
 #pragma unroll
                 for (int k = 0; k < 4; k++)
-                  y[4 * i + k] = (v == 0 ? 0u : pv[k] - f.base) + zz_dec(y[4 * i + k]);
+                  y[4 * i + k] = (v == 0 ? 0u : pv[k] - f.base) + (f.zz ? zz_dec(y[4 * i + k]) : y[4 * i + k]);
               }
             }
 #pragma unroll

@@ -14,12 +14,12 @@
 // The thread path takes the common blocks only: a valid header of integer
 // type 1 or 2, a full block (128 values) whose length and count agree with
 // the batch's tables, at most 16 exceptions in strictly increasing
-// positions, exceptions only without delta, delta only with zigzag (no
-// overflow is possible).  Every other block -- bitmap exceptions, plain
-// delta (whose overflow position must be reported), partial or corrupt
-// blocks -- goes to the quad decoder (utl_quad.cuh) after the tile's rows
-// are out, from the same staged bytes, which reports the reference's exact
-// status.  Decode steps follow unpackUint32Scalar (scalar.go:260-309),
+// positions, exceptions only without delta, plain (not zigzag) delta only
+// at widths whose sums cannot wrap (no overflow is possible, so no block
+// the thread path takes can fail).  Every other block -- bitmap
+// exceptions, delta with exceptions, partial or corrupt blocks -- goes to
+// the quad decoder (utl_quad.cuh) after the tile's rows are out, from the
+// same staged bytes, which reports the reference's exact status.  Decode steps follow unpackUint32Scalar (scalar.go:260-309),
 // decodeUnpackHeader (unpack_block.go:62-172), applyExceptions
 // (exceptions.go:194-284) and deltaDecodePerLane* (delta.go:50-115).
 #pragma once
@@ -38,7 +38,7 @@ constexpr int kBlocksPerStore = 32 / kLanesPerBlock;
 struct Plan {
   int bw, exc, nc, pay, xo, svb;
   uint32_t base, cw, mask;
-  bool delta;
+  bool delta, zz;
 };
 
 // Whether the block at staging offset blk (len bytes; want values expected)
@@ -57,7 +57,10 @@ __device__ __forceinline__ bool plan(const SmemBytes& sb, int blk, int len, int 
   const bool delta = (h & kHdrDelta) != 0, zz = (h & kHdrZigZag) != 0;
   // unpack_block.go:62-172: type, count and width; exceptions in list mode
   if (!(itype == 1 || itype == 2) || count != kBlock || bwf > 8 || exc > 16) return false;
-  if (delta && (exc > 0 || !zz)) return false;
+  // plain delta: at width 28 or less eight values cannot wrap a uint32 sum
+  // (so no overflow to report); delta blocks with exceptions go to the quads
+  if (delta && (exc > 0 || (!zz && bwf > 7))) return false;
+  f.zz = zz;
   f.bw = 4 * bwf;
   f.exc = exc;
   f.delta = delta;
