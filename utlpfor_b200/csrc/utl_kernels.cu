@@ -2196,6 +2196,9 @@ __device__ __forceinline__ void lane_take_and_plan(const PackArgs& a, const Lane
 // 32 readable bytes past len.
 template <int Q>
 __device__ __forceinline__ void lane_copy_chunks(const uint4* img4, uint4* dst, int nf, int b, int lane) {
+  // unrolled: several chunks' shared loads in flight before their stores
+  // (measured c3 pack 0.535 -> 0.506 ms)
+#pragma unroll 4
   for (int i = lane; i < nf; i += 32) {
     const uint4 I0 = img4[i], I1 = img4[i + 1];
     const uint32_t v[8] = {I0.x, I0.y, I0.z, I0.w, I1.x, I1.y, I1.z, I1.w};
